@@ -1,0 +1,140 @@
+/*
+ * radik.h -- C ABI of the B200 (sm_100a) exact Float32 radix top-k engine.
+ *
+ * Drop-in boundary for RadiK.jl (WilliBee/RadiK.jl v0.1.3).  Each entry point
+ * names the reference interface it replaces (paths relative to the RadiK.jl
+ * project root).  All array arguments are raw pointers:
+ *   d_*  device memory (CUDA global memory of the current device),
+ *   h_*  host memory.
+ * Layouts follow the Julia API: the input is the concatenation of all tasks
+ * (Float32, task t occupies [off_t, off_t + task_lens[t])), outputs are
+ * column-major [k, num_tasks] arrays, i.e. task t's k results are contiguous
+ * at t*k.  Indices are 4- or 8-byte signed integers (Int32 / Int64);
+ * automatic indices are 1-based positions inside each task, custom indices
+ * are copied from indices[global position]; short tasks are padded with value
+ * 0 and index -1.  `stream` is a cudaStream_t (NULL = legacy default stream).
+ *
+ * Every function returns a radik_status; radik_last_error() holds the message
+ * of the last failure on the calling thread (the text of the reference's
+ * error(...) where one exists).
+ */
+#ifndef RADIK_B200_H
+#define RADIK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum radik_status {
+    RADIK_OK = 0,
+    RADIK_ERR_INVALID = 1,        /* bad argument (Julia: ErrorException)          */
+    RADIK_ERR_OOM = 2,            /* device or host allocation failed              */
+    RADIK_ERR_WS_TOO_SMALL = 3,   /* workspace cannot hold the call                */
+    RADIK_ERR_CUDA = 4,           /* a CUDA runtime call failed                    */
+    RADIK_ERR_DEVICE = 5,         /* a kernel reported an error (see radik_ws_error) */
+    RADIK_ERR_TIMEOUT = 6,        /* a bounded device wait gave up                 */
+    RADIK_ERR_CAPTURE = 7         /* operation not allowed while the stream captures */
+} radik_status;
+
+/* Flags of topk_radix_select! (src/algorithm.jl:170-175: Val(LARGEST),
+ * Val(ASCEND), Val(WITHSCALE), Val(WITHIDXIN), Val(WITHPACKING)). */
+#define RADIK_LARGEST     0x1u
+#define RADIK_ASCEND      0x2u
+#define RADIK_WITHSCALE   0x4u
+#define RADIK_WITHIDXIN   0x8u
+#define RADIK_WITHPACKING 0x10u   /* accepted for parity; loads are always 128-bit */
+/* Engine flags (no reference counterpart). */
+#define RADIK_ASYNC       0x100u  /* return after enqueueing; no host synchronisation */
+#define RADIK_PLAIN       0x200u  /* use the multi-pass per-call path (reference shape) */
+
+typedef struct radik_ws radik_ws;
+
+/* RadiKWorkspace(backend, n, num_tasks, I=Int32), src/algorithm.jl:58-83.
+ * n: longest task the workspace serves; num_tasks: largest batch;
+ * index_bytes: width of the workspace integer type I (4 or 8).  Device
+ * buffers grow on first use with a larger k; prepare before graph capture. */
+int radik_ws_create(int64_t n, int64_t num_tasks, int index_bytes, radik_ws** ws);
+int radik_ws_destroy(radik_ws* ws);
+/* Device bytes currently held by the workspace. */
+int radik_ws_bytes(const radik_ws* ws, size_t* bytes);
+/* Synchronises the workspace's last stream, returns and clears the device
+ * error word (bit 0 capacity, 1 bounds, 2 timeout, 3 internal). */
+int radik_ws_error(radik_ws* ws, uint32_t* bits);
+
+/* Builds (and caches in ws) the launch plan for this batch shape: segment
+ * table, kernel choice, buffer sizes.  Calls with the same shape reuse it and
+ * enqueue only kernels and memsets, so they can be captured in CUDA graphs. */
+int radik_ws_prepare(radik_ws* ws, const int64_t* h_task_lens, int64_t num_tasks, int64_t k, uint32_t flags,
+                     int idx_bytes);
+
+/* topk_radix_select!(val_out, idx_out, ws, val_in, idx_in, task_lens, k,
+ *                    Val(LARGEST), Val(ASCEND), Val(WITHSCALE), Val(WITHIDXIN),
+ *                    Val(WITHPACKING), Val(VLOAD_SIZE_BYTES))
+ * src/algorithm.jl:162-368.  Requires max(task_lens) <= ws n and
+ * num_tasks <= ws num_tasks (src/algorithm.jl:156-160).  d_idx_in is read only
+ * with RADIK_WITHIDXIN.  Synchronous (like the reference, :353) unless
+ * RADIK_ASYNC is set. */
+int radik_topk_radix_select(float* d_val_out, void* d_idx_out, int idx_bytes, radik_ws* ws,
+                            const float* d_val_in, const void* d_idx_in, const int64_t* h_task_lens,
+                            int64_t num_tasks, int64_t k, uint32_t flags, void* stream);
+
+/* topk!(val_out, idx_out, data, task_lens, k; indices, largest, rev),
+ * src/algorithm.jl:477-522: validates the index length (:506-510), allocates a
+ * fresh workspace for the call (:503), runs with ASCEND = !rev (:520) and
+ * returns when the results are complete.  d_indices may be NULL
+ * (indices_len 0) for automatic indices. */
+int radik_topk(float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_data, int64_t data_len,
+               const void* d_indices, int64_t indices_len, const int64_t* h_task_lens, int64_t num_tasks,
+               int64_t k, int largest, int rev, void* stream);
+
+/* Same as radik_topk with HOST buffers: copies the input (and indices) to
+ * the device, runs, copies the results back.  h_data may be pinned or
+ * pageable. */
+int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const float* h_data, int64_t data_len,
+                    const void* h_indices, int64_t indices_len, const int64_t* h_task_lens, int64_t num_tasks,
+                    int64_t k, int largest, int rev, radik_ws* ws, void* stream);
+
+/* ---- Stage entry points: the reference kernels' own contracts ----------- */
+
+/* count_bin_ex_kernel!, src/kernels/count_bin.jl:78-203: per-task histogram
+ * of get_bin_id(apply_scaling(v), LEFT, RIGHT) over the concatenated tasks
+ * (NaN skipped).  d_hist: int32 [num_tasks][2^(32-RIGHT)], overwritten. */
+int radik_count_bin_ex(int32_t* d_hist, const float* d_data, const int64_t* h_task_lens, int64_t num_tasks,
+                       int left, int right, int withscale, int largest, void* stream);
+
+/* count_bin_kernel!, src/kernels/count_bin.jl:20-59: padded layout
+ * d_data[t*stride + i], i < task_lens[t]. */
+int radik_count_bin(int32_t* d_hist, const float* d_data, const int64_t* h_task_lens, int64_t stride,
+                    int64_t num_tasks, int left, int right, void* stream);
+
+/* select_bin_kernel!, src/kernels/select_bin.jl:268-348: per task, the
+ * 1-based bin holding rank k_values[t] (from the top bin when largest),
+ * the residual rank and the bin's count; entries are left unchanged when the
+ * rank is out of range.  d_hist int32 [num_tasks][hist_len]. */
+int radik_select_bin(int32_t* d_bin_ids, int32_t* d_k_values, int32_t* d_counts, const int32_t* d_hist,
+                     int64_t num_tasks, int64_t hist_len, int largest, void* stream);
+
+/* filter_kernel! / filter_general_kernel!, src/kernels/filter.jl:172-621:
+ * emits (value, index) for elements strictly better than d_kth[t] and, for
+ * elements equal to it, while the boundary counter d_boundary[t] stays >= 0
+ * after decrement; tasks with len <= k copy everything.  Output rows have
+ * stride k; d_counts[t] receives the number emitted (emission order is
+ * unspecified, as in the reference). */
+int radik_filter(float* d_val_out, void* d_idx_out, int idx_bytes, int32_t* d_counts, int32_t* d_boundary,
+                 const float* d_data, const void* d_idx_in, const float* d_kth, const int64_t* h_task_lens,
+                 int64_t num_tasks, int64_t k, int withscale, int largest, void* stream);
+
+/* Message of the last failure on this thread ("" when none). */
+const char* radik_last_error(void);
+const char* radik_status_string(int status);
+/* Library version string. */
+const char* radik_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RADIK_B200_H */

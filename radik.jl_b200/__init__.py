@@ -1,0 +1,328 @@
+"""radik.jl_b200 -- Python host side of the B200 exact Float32 radix top-k.
+
+This module mirrors RadiK.jl's public API (src/RadiK.jl:19-22 exports
+``topk_radix_select!``, ``topk``, ``topk!``, ``RadiKWorkspace``) over the C ABI
+of libradik_b200.so (include/radik.h).  Device arrays are CUDA torch tensors
+(torch is used only for device memory and streams); every computation runs in
+the library's sm_100a kernels and there is no CPU fallback.
+
+Layout: Julia's column-major ``[k, num_tasks]`` outputs are torch tensors of
+shape ``(num_tasks, k)`` (the same memory), the input is the concatenation of
+all tasks.  Julia's ``!`` suffix becomes a trailing underscore:
+
+    topk(data, k; indices, largest, rev)                -> topk(data, k, ...)
+    topk(data, task_lens, k; ...)                       -> topk(data, task_lens, k, ...)
+    topk!(val_out, idx_out, data, [task_lens,] k; ...)  -> topk_(val_out, idx_out, data, [task_lens,] k, ...)
+    topk_radix_select!(val_out, idx_out, ws, val_in, idx_in, task_lens, k,
+                       Val(LARGEST), Val(ASCEND), Val(WITHSCALE), Val(WITHIDXIN), ...)
+                                                        -> topk_radix_select_(...)
+    RadiKWorkspace(backend, n, num_tasks, I=Int32)      -> RadiKWorkspace(backend, n, num_tasks, I=torch.int32)
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Sequence
+
+import numpy as np
+
+from ._lib import (RADIK_ASCEND, RADIK_ASYNC, RADIK_LARGEST, RADIK_PLAIN, RADIK_WITHIDXIN,
+                   RADIK_WITHPACKING, RADIK_WITHSCALE, RadiKError, check, load)
+
+__all__ = ["topk", "topk_", "topk_radix_select_", "RadiKWorkspace", "RadiKError", "topk_host",
+           "count_bin_ex", "count_bin", "select_bin", "filter_", "version"]
+
+
+def _torch():
+    import torch  # deferred: the library loads without torch
+    return torch
+
+
+def version() -> str:
+    return load().radik_version().decode()
+
+
+def _ptr(t) -> ctypes.c_void_p | None:
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream) -> ctypes.c_void_p:
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def _lens_array(task_lens) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(task_lens, dtype=np.int64).reshape(-1))
+    return a
+
+
+def _check_cuda(t, what: str):
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise RadiKError(f"{what} must be a CUDA tensor (the engine has no CPU path)")
+    if not t.is_contiguous():
+        raise RadiKError(f"{what} must be contiguous")
+
+
+def _check_float32(data):
+    torch = _torch()
+    if data.dtype != torch.float32:
+        # src/algorithm.jl:492-494
+        raise RadiKError(f"RadiK.jl only supports Float32 input data. Got {data.dtype}. "
+                         "Convert with: data.to(torch.float32)")
+
+
+def _idx_bytes(dtype) -> int:
+    torch = _torch()
+    if dtype == torch.int32:
+        return 4
+    if dtype == torch.int64:
+        return 8
+    raise RadiKError(f"index type must be Int32 or Int64, got {dtype}")
+
+
+class RadiKWorkspace:
+    """Device workspace, RadiKWorkspace(backend, n, num_tasks, I) in
+    src/algorithm.jl:58-83.  ``n`` bounds the longest task and ``num_tasks``
+    the batch of every call that uses it (src/algorithm.jl:156-160).  The
+    engine sizes its buffers from the calls it serves; ``I`` is kept for API
+    parity (4- or 8-byte integers)."""
+
+    def __init__(self, backend, n: int, num_tasks: int, I=None):
+        torch = _torch()
+        self.backend = backend
+        self.n = int(n)
+        self.num_tasks = int(num_tasks)
+        self.I = torch.int32 if I is None else I
+        self.device = torch.device("cuda", torch.cuda.current_device()) if backend in (None, "cuda") else \
+            torch.device(backend)
+        L = load()
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            check(L.radik_ws_create(self.n, self.num_tasks, _idx_bytes(self.I), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def nbytes(self) -> int:
+        b = ctypes.c_size_t()
+        check(load().radik_ws_bytes(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+    def error_bits(self) -> int:
+        b = ctypes.c_uint32()
+        check(load().radik_ws_error(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+    def prepare(self, task_lens, k: int, *, largest=True, ascend=True, withscale=False,
+                withidxin=False, idx_dtype=None, plain=False) -> None:
+        """Build the launch plan for a batch shape ahead of CUDA-graph capture."""
+        torch = _torch()
+        lens = _lens_array(task_lens)
+        flags = _flags(largest, ascend, withscale, withidxin, plain)
+        ib = _idx_bytes(idx_dtype if idx_dtype is not None else torch.int32)
+        check(load().radik_ws_prepare(self._h, lens.ctypes.data_as(ctypes.c_void_p), len(lens), int(k),
+                                      flags, ib))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load().radik_ws_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _flags(largest, ascend, withscale, withidxin, plain=False, sync=True) -> int:
+    f = RADIK_WITHPACKING
+    f |= RADIK_LARGEST if largest else 0
+    f |= RADIK_ASCEND if ascend else 0
+    f |= RADIK_WITHSCALE if withscale else 0
+    f |= RADIK_WITHIDXIN if withidxin else 0
+    f |= RADIK_PLAIN if plain else 0
+    f |= 0 if sync else RADIK_ASYNC
+    return f
+
+
+def topk_radix_select_(val_out, idx_out, ws: RadiKWorkspace, val_in, idx_in, task_lens, k: int,
+                       largest: bool = True, ascend: bool = True, withscale: bool = False,
+                       withidxin: bool = False, withpacking: bool = True, vload_size_bytes: int = 32,
+                       *, stream=None, plain: bool = False, sync: bool = True):
+    """topk_radix_select!(val_out, idx_out, ws, val_in, idx_in, task_lens, k,
+    Val(LARGEST), Val(ASCEND), Val(WITHSCALE), Val(WITHIDXIN), Val(WITHPACKING),
+    Val(VLOAD_SIZE_BYTES)) -- src/algorithm.jl:162-368.
+
+    Writes the k selected values/indices of every task into val_out/idx_out
+    ((num_tasks, k) tensors), sorted ascending when ``ascend``.  Synchronous
+    like the reference unless ``sync=False``.  ``withpacking`` and
+    ``vload_size_bytes`` are accepted for parity (loads are 128-bit)."""
+    _check_cuda(val_out, "val_out")
+    _check_cuda(idx_out, "idx_out")
+    _check_cuda(val_in, "val_in")
+    _check_float32(val_in)
+    if withidxin:
+        _check_cuda(idx_in, "idx_in")
+        if idx_in.dtype != idx_out.dtype:
+            raise RadiKError("idx_in and idx_out must have the same element type")
+    lens = _lens_array(task_lens)
+    L = load()
+    flags = _flags(largest, ascend, withscale, withidxin, plain, sync)
+    check(L.radik_topk_radix_select(_ptr(val_out), _ptr(idx_out), _idx_bytes(idx_out.dtype), ws.handle,
+                                    _ptr(val_in), _ptr(idx_in) if withidxin else None,
+                                    lens.ctypes.data_as(ctypes.c_void_p), len(lens), int(k), flags,
+                                    _stream(stream)))
+    return val_out, idx_out
+
+
+def _split_args(task_lens_or_k, k, data):
+    if k is None:
+        return [int(data.numel())], int(task_lens_or_k), True
+    return list(np.asarray(task_lens_or_k, dtype=np.int64).reshape(-1)), int(k), False
+
+
+def topk_(val_out, idx_out, data, task_lens_or_k, k=None, *, indices=None, largest=True, rev=False,
+          stream=None, plain=False):
+    """topk!(val_out, idx_out, data, [task_lens,] k; indices, largest, rev) --
+    src/algorithm.jl:477-526.  Validates sizes, uses a fresh workspace for the
+    call (as the reference does, :503) and returns when the results are
+    complete.  ``rev=False`` sorts the selected values ascending (:520)."""
+    _check_float32(data)
+    task_lens, k, single = _split_args(task_lens_or_k, k, data)
+    T = len(task_lens)
+    expected = (k,) if (single and val_out.dim() == 1) else (T, k)
+    # src/algorithm.jl:497-501
+    if tuple(val_out.shape) != expected:
+        raise RadiKError(f"val_out must have size {expected}, got {tuple(val_out.shape)}")
+    if tuple(idx_out.shape) != expected:
+        raise RadiKError(f"idx_out must have size {expected}, got {tuple(idx_out.shape)}")
+    # src/algorithm.jl:506-510
+    if indices is not None and indices.numel() > 0 and indices.numel() != data.numel():
+        raise RadiKError("indices length must equal data length. "
+                         f"Got {indices.numel()} vs {data.numel()}")
+    with_idx = indices is not None and indices.numel() > 0
+    ws = RadiKWorkspace("cuda", max(task_lens) if T else 0, T)
+    try:
+        topk_radix_select_(val_out, idx_out, ws, data, indices if with_idx else None, task_lens, k,
+                           largest, not rev, False, with_idx, True, stream=stream, plain=plain)
+    finally:
+        ws.close()
+    return None
+
+
+def topk(data, task_lens_or_k, k=None, *, indices=None, largest=True, rev=False, stream=None,
+         plain=False):
+    """topk(data, k; ...) -> (values[k], indices[k]) and topk(data, task_lens, k; ...)
+    -> (values[T, k], indices[T, k]) -- src/algorithm.jl:528-559.  The index
+    type follows ``indices`` (default Int32)."""
+    torch = _torch()
+    _check_float32(data)
+    task_lens, kk, single = _split_args(task_lens_or_k, k, data)
+    T = len(task_lens)
+    idx_dtype = torch.int32 if indices is None else indices.dtype
+    val_out = torch.zeros((T, kk), dtype=torch.float32, device=data.device)
+    idx_out = torch.zeros((T, kk), dtype=idx_dtype, device=data.device)
+    topk_(val_out, idx_out, data, task_lens, kk, indices=indices, largest=largest, rev=rev,
+          stream=stream, plain=plain)
+    if single:
+        return val_out[0], idx_out[0]
+    return val_out, idx_out
+
+
+def topk_host(data: np.ndarray, task_lens: Sequence[int], k: int, *, indices: np.ndarray | None = None,
+              largest=True, rev=False, ws: RadiKWorkspace | None = None, stream=None,
+              out: tuple[np.ndarray, np.ndarray] | None = None):
+    """Top-k of HOST (numpy) buffers through radik_topk_host: copies in,
+    selects on the GPU, copies the (T, k) results back."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    lens = _lens_array(task_lens)
+    T = len(lens)
+    idx_dtype = np.int32 if indices is None else np.asarray(indices).dtype
+    if out is None:
+        vo = np.zeros((T, k), np.float32)
+        io = np.zeros((T, k), idx_dtype)
+    else:
+        vo, io = out
+    own = ws is None
+    if own:
+        ws = RadiKWorkspace("cuda", int(lens.max()) if T else 0, T)
+    try:
+        ind = None if indices is None else np.ascontiguousarray(indices)
+        check(load().radik_topk_host(vo.ctypes.data_as(ctypes.c_void_p), io.ctypes.data_as(ctypes.c_void_p),
+                                     io.dtype.itemsize, data.ctypes.data_as(ctypes.c_void_p), data.size,
+                                     None if ind is None else ind.ctypes.data_as(ctypes.c_void_p),
+                                     0 if ind is None else ind.size, lens.ctypes.data_as(ctypes.c_void_p), T,
+                                     int(k), int(bool(largest)), int(bool(rev)), ws.handle, _stream(stream)))
+    finally:
+        if own:
+            ws.close()
+    return vo, io
+
+
+# ---- stage entry points (the reference kernels' contracts) -----------------
+
+def count_bin_ex(data, task_lens, left: int, right: int, withscale=False, largest=True, stream=None):
+    """count_bin_ex_kernel! (src/kernels/count_bin.jl:78-203) -> int32 (T, 2^(32-right))."""
+    torch = _torch()
+    _check_cuda(data, "data")
+    lens = _lens_array(task_lens)
+    hist = torch.zeros((len(lens), 1 << (32 - right)), dtype=torch.int32, device=data.device)
+    check(load().radik_count_bin_ex(_ptr(hist), _ptr(data), lens.ctypes.data_as(ctypes.c_void_p), len(lens),
+                                    left, right, int(withscale), int(largest), _stream(stream)))
+    return hist
+
+
+def count_bin(padded, task_lens, stride: int, left: int, right: int, stream=None):
+    """count_bin_kernel! (src/kernels/count_bin.jl:20-59) on the padded layout."""
+    torch = _torch()
+    _check_cuda(padded, "data")
+    lens = _lens_array(task_lens)
+    hist = torch.zeros((len(lens), 1 << (32 - right)), dtype=torch.int32, device=padded.device)
+    check(load().radik_count_bin(_ptr(hist), _ptr(padded), lens.ctypes.data_as(ctypes.c_void_p), int(stride),
+                                 len(lens), left, right, _stream(stream)))
+    return hist
+
+
+def select_bin(hist, k_values, largest: bool, bin_ids=None, counts=None, stream=None):
+    """select_bin_kernel! (src/kernels/select_bin.jl:268-348) -> (bin_ids 1-based,
+    residual k_values, counts); entries stay unchanged when k is out of range."""
+    torch = _torch()
+    _check_cuda(hist, "hist")
+    T, hl = hist.shape
+    kv = torch.as_tensor(np.asarray(k_values, np.int32), device=hist.device).clone()
+    bi = torch.zeros(T, dtype=torch.int32, device=hist.device) if bin_ids is None else \
+        torch.as_tensor(np.asarray(bin_ids, np.int32), device=hist.device).clone()
+    ct = torch.zeros(T, dtype=torch.int32, device=hist.device) if counts is None else \
+        torch.as_tensor(np.asarray(counts, np.int32), device=hist.device).clone()
+    check(load().radik_select_bin(_ptr(bi), _ptr(kv), _ptr(ct), _ptr(hist.contiguous()), T, hl, int(largest),
+                                  _stream(stream)))
+    return bi, kv, ct
+
+
+def filter_(data, task_lens, kth, boundary, k: int, withscale=False, largest=True, idx_in=None,
+            idx_dtype=None, stream=None):
+    """filter_kernel! / filter_general_kernel! (src/kernels/filter.jl:172-621).
+    Returns per-task (values, indices) in emission order and the counters."""
+    torch = _torch()
+    _check_cuda(data, "data")
+    lens = _lens_array(task_lens)
+    T = len(lens)
+    dev = data.device
+    idt = idx_in.dtype if idx_in is not None else (idx_dtype or torch.int32)
+    width = max(int(k), 1)
+    vo = torch.zeros((T, width), dtype=torch.float32, device=dev)
+    io = torch.zeros((T, width), dtype=idt, device=dev)
+    cnt = torch.zeros(T, dtype=torch.int32, device=dev)
+    bnd = torch.as_tensor(np.asarray(boundary, np.int32), device=dev).clone()
+    kt = torch.as_tensor(np.asarray(kth, np.float32), device=dev).clone()
+    check(load().radik_filter(_ptr(vo), _ptr(io), _idx_bytes(idt), _ptr(cnt), _ptr(bnd), _ptr(data),
+                              _ptr(idx_in), _ptr(kt), lens.ctypes.data_as(ctypes.c_void_p), T, int(k),
+                              int(withscale), int(largest), _stream(stream)))
+    c = cnt.cpu().numpy()
+    v, i = vo.cpu().numpy(), io.cpu().numpy()
+    return [(v[t, :c[t]], i[t, :c[t]]) for t in range(T)], bnd.cpu().numpy()

@@ -1,0 +1,742 @@
+// api.cu -- C ABI of the engine (include/radik.h): workspace, launch plans,
+// the fused single-read path, the multi-pass path and the stage entry points.
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/radik.h"
+#include "fused.cuh"
+#include "general.cuh"
+#include "stages.cuh"
+
+using namespace radik;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define RADIK_CUDA(call)                                                                         \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) return fail(RADIK_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t b) {
+        if (b <= bytes) return cudaSuccess;
+        if (p) { cudaFree(p); p = nullptr; bytes = 0; }
+        size_t nb = b < 256 ? 256 : b;
+        cudaError_t e = cudaMalloc(&p, nb);
+        if (e == cudaSuccess) bytes = nb;
+        return e;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    template <typename T> T* as(size_t byte_off = 0) const {
+        return reinterpret_cast<T*>(static_cast<char*>(p) + byte_off);
+    }
+};
+
+struct DeviceInfo {
+    int sms = 148;
+    int max_smem_optin = 227 * 1024;
+};
+
+DeviceInfo device_info() {
+    static std::mutex mu;
+    static int cached_dev = -1;
+    static DeviceInfo cached;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev != cached_dev) {
+        DeviceInfo d;
+        cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&d.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        cached = d;
+        cached_dev = dev;
+    }
+    return cached;
+}
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// ---------------------------------------------------------------------------
+// Fused kernel dispatch
+// ---------------------------------------------------------------------------
+using FusedKernel = void (*)(FusedParams);
+
+template <int T, int V, bool S>
+FusedKernel fused_ptr() { return fused_topk_kernel<T, V, S>; }
+
+FusedKernel pick_fused(int threads, int vec, bool scale) {
+    if (threads == 256 && vec == 8) return scale ? fused_ptr<256, 8, true>() : fused_ptr<256, 8, false>();
+    if (threads == 256 && vec == 16) return scale ? fused_ptr<256, 16, true>() : fused_ptr<256, 16, false>();
+    if (threads == 512 && vec == 8) return scale ? fused_ptr<512, 8, true>() : fused_ptr<512, 8, false>();
+    if (threads == 512 && vec == 16) return scale ? fused_ptr<512, 16, true>() : fused_ptr<512, 16, false>();
+    return nullptr;
+}
+
+int env_int(const char* name, int dflt) {
+    const char* v = std::getenv(name);
+    return (v && *v) ? std::atoi(v) : dflt;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Workspace and plan
+// ---------------------------------------------------------------------------
+struct PlanKey {
+    std::vector<int64_t> lens;
+    int64_t k = -1;
+    uint32_t flags = 0;
+    int idx_bytes = 0;
+    bool operator==(const PlanKey& o) const {
+        return k == o.k && flags == o.flags && idx_bytes == o.idx_bytes && lens == o.lens;
+    }
+};
+
+struct Plan {
+    PlanKey key;
+    bool valid = false;
+    bool fused = false;
+    int threads = 256, vec = 16;
+    uint32_t cap = 0;
+    int grid = 0;
+    size_t smem = 0;
+    int64_t T = 0, N = 0, slots = 0;
+    int32_t nsegs = 0;
+    std::vector<FusedTask> tasks;
+    std::vector<FusedSeg> segs;
+};
+
+struct radik_ws {
+    int device = 0;
+    int64_t n = 0;          // longest task served (RadiKWorkspace n)
+    int64_t num_tasks = 0;  // largest batch (RadiKWorkspace num_tasks)
+    int index_bytes = 4;
+    cudaStream_t last_stream = nullptr;
+    uint32_t* h_err = nullptr;  // pinned
+    DevBuf state;     // [err, work_counter, any, pad] + gthr[T] + task_done[T]
+    DevBuf desc;      // tasks + segs of the plan
+    DevBuf cand;      // fused: slots * k composites
+    DevBuf slot_cnt;  // fused: slots
+    DevBuf scratch;   // sort scratch
+    DevBuf hist;      // plain: [T][4096]
+    DevBuf pstate;    // plain: [T] PlainState
+    DevBuf stage;     // plain: [T][k]
+    DevBuf pcand[2];  // plain: [N] each
+    DevBuf io_in, io_idx, io_vout, io_iout;  // host-buffer entry point
+    Plan plan;
+};
+
+namespace {
+
+constexpr size_t kStateHeader = 16;
+
+uint32_t* err_ptr(radik_ws* ws) { return ws->state.as<uint32_t>(0); }
+
+// Build the launch plan for a batch shape (host only).
+int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes) {
+    Plan& pl = ws->plan;
+    PlanKey key;
+    key.lens.assign(lens, lens + T);
+    key.k = k;
+    key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
+    key.idx_bytes = idx_bytes;
+    if (pl.valid && pl.key == key) return RADIK_OK;
+
+    const DeviceInfo di = device_info();
+    Plan np;
+    np.key = key;
+    np.T = T;
+    np.N = 0;
+    for (int64_t t = 0; t < T; ++t) np.N += lens[t];
+
+    // Fused configuration: the shared buffer must hold k + one tile.
+    np.threads = env_int("RADIK_THREADS", 256);
+    int64_t avg = T > 0 ? np.N / T : 0;
+    np.vec = env_int("RADIK_VEC", (avg >= (1 << 16)) ? 16 : 8);
+    const bool scale = (flags & RADIK_WITHSCALE) != 0;
+    FusedKernel fk = pick_fused(np.threads, np.vec, scale);
+    if (!fk) return fail(RADIK_ERR_INVALID, "unsupported RADIK_THREADS/RADIK_VEC combination");
+    const size_t tile = static_cast<size_t>(np.threads) * np.vec;
+    size_t kk = static_cast<size_t>(k);
+    size_t cap = kk + tile + 8;
+    size_t p2 = 1;
+    while (p2 < std::min<size_t>(kk, kBitonicMax)) p2 <<= 1;
+    cap = std::max(cap, p2);
+    cap = std::max(cap, kk + (static_cast<size_t>(np.threads) / 32 * 256 + 256) / 2 + 8);
+    cap = round_up(cap, 64);
+    np.cap = static_cast<uint32_t>(cap);
+    np.smem = cap * sizeof(uint64_t);
+    np.fused = (flags & RADIK_PLAIN) == 0 && np.smem <= static_cast<size_t>(di.max_smem_optin) - 2048;
+
+    int occ = 1;
+    if (np.fused) {
+        static std::mutex attr_mu;
+        {
+            std::lock_guard<std::mutex> lock(attr_mu);
+            cudaFuncSetAttribute(reinterpret_cast<const void*>(fk), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(np.smem));
+        }
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fk, np.threads, np.smem) != cudaSuccess || occ < 1)
+            occ = 1;
+    }
+    const int64_t resident = static_cast<int64_t>(occ) * di.sms;
+
+    // Segments: tasks longer than seg_len are split (the last segment of a
+    // task may be shorter); segment boundaries stay 16-byte aligned relative
+    // to the task start.
+    int64_t seg_len = env_int("RADIK_SEG", 0);
+    if (seg_len <= 0) {
+        int64_t target = np.N / std::max<int64_t>(1, 3 * resident);
+        seg_len = std::max<int64_t>(64 * static_cast<int64_t>(tile), target);
+    }
+    seg_len = static_cast<int64_t>(round_up(static_cast<size_t>(seg_len), tile));
+    if (!np.fused) seg_len = std::max<int64_t>(seg_len, 1 << 20);
+    np.tasks.resize(T);
+    np.segs.clear();
+    np.slots = 0;
+    int64_t off = 0;
+    for (int64_t t = 0; t < T; ++t) {
+        FusedTask& td = np.tasks[t];
+        td.start = off;
+        td.len = lens[t];
+        int64_t nseg = 1;
+        if (np.fused && td.len > seg_len && td.len > k) nseg = (td.len + seg_len - 1) / seg_len;
+        if (!np.fused) nseg = std::max<int64_t>(1, (td.len + seg_len - 1) / seg_len);
+        td.nseg = static_cast<int32_t>(nseg);
+        td.slot0 = (np.fused && nseg > 1) ? np.slots : -1;
+        if (np.fused && nseg > 1) np.slots += nseg;
+        for (int64_t s = 0; s < nseg; ++s) {
+            FusedSeg sg;
+            sg.start = off + s * seg_len;
+            int64_t e = std::min(td.len, (s + 1) * seg_len);
+            sg.len = static_cast<int32_t>(e - s * seg_len);
+            sg.task = static_cast<int32_t>(t);
+            sg.seg_in_task = static_cast<int32_t>(s);
+            sg.pad_ = 0;
+            np.segs.push_back(sg);
+        }
+        off += td.len;
+    }
+    // Longest work first (uneven batches), stable on task order.
+    std::stable_sort(np.segs.begin(), np.segs.end(),
+                     [](const FusedSeg& a, const FusedSeg& b) { return a.len > b.len; });
+    np.nsegs = static_cast<int32_t>(np.segs.size());
+    np.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(np.nsegs, resident)));
+    np.valid = true;
+
+    // Device buffers.
+    const size_t state_bytes = kStateHeader + round_up(sizeof(uint64_t) * T, 16) + sizeof(uint32_t) * T;
+    const size_t desc_bytes = round_up(sizeof(FusedTask) * T, 256) + sizeof(FusedSeg) * np.segs.size();
+    cudaError_t e = ws->state.ensure(state_bytes);
+    if (e == cudaSuccess) e = ws->desc.ensure(desc_bytes);
+    if (e == cudaSuccess && np.fused) {
+        e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.slots) * kk);
+        if (e == cudaSuccess) e = ws->slot_cnt.ensure(sizeof(uint32_t) * static_cast<size_t>(np.slots));
+        if (e == cudaSuccess && kk > kBitonicMax)
+            e = ws->scratch.ensure(sizeof(uint64_t) * static_cast<size_t>(np.grid) * kk);
+    }
+    if (e == cudaSuccess && !np.fused) {
+        e = ws->hist.ensure(sizeof(uint32_t) * 4096 * static_cast<size_t>(T));
+        if (e == cudaSuccess) e = ws->pstate.ensure(sizeof(PlainState) * static_cast<size_t>(T));
+        if (e == cudaSuccess) e = ws->stage.ensure(sizeof(uint64_t) * static_cast<size_t>(T) * kk);
+        if (e == cudaSuccess) e = ws->pcand[0].ensure(sizeof(uint64_t) * static_cast<size_t>(np.N));
+        if (e == cudaSuccess) e = ws->pcand[1].ensure(sizeof(uint64_t) * static_cast<size_t>(np.N));
+        if (e == cudaSuccess && kk > kBitonicMax)
+            e = ws->scratch.ensure(sizeof(uint64_t) * static_cast<size_t>(T) * kk);
+    }
+    if (e != cudaSuccess) {
+        pl.valid = false;
+        return fail(e == cudaErrorMemoryAllocation ? RADIK_ERR_OOM : RADIK_ERR_CUDA,
+                    std::string("workspace allocation: ") + cudaGetErrorString(e));
+    }
+    e = cudaMemcpy(ws->desc.p, np.tasks.data(), sizeof(FusedTask) * T, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !np.segs.empty())
+        e = cudaMemcpy(ws->desc.as<char>(round_up(sizeof(FusedTask) * T, 256)), np.segs.data(),
+                       sizeof(FusedSeg) * np.segs.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, state_bytes);
+    if (e != cudaSuccess) {
+        pl.valid = false;
+        return fail(RADIK_ERR_CUDA, std::string("plan upload: ") + cudaGetErrorString(e));
+    }
+    pl = std::move(np);
+    return RADIK_OK;
+}
+
+const FusedTask* plan_tasks(radik_ws* ws) { return ws->desc.as<FusedTask>(0); }
+const FusedSeg* plan_segs(radik_ws* ws) {
+    return ws->desc.as<FusedSeg>(round_up(sizeof(FusedTask) * ws->plan.T, 256));
+}
+
+FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, const float* vin, const void* iin,
+                         int64_t k, uint32_t flags) {
+    const Plan& pl = ws->plan;
+    FusedParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.data = vin;
+    p.tasks = plan_tasks(ws);
+    p.segs = plan_segs(ws);
+    p.nsegs = pl.nsegs;
+    p.k = static_cast<uint32_t>(k);
+    p.cap = pl.cap;
+    p.ascend = (flags & RADIK_ASCEND) ? 1 : 0;
+    p.sp = make_score_params((flags & RADIK_LARGEST) != 0, (flags & RADIK_WITHSCALE) != 0);
+    p.idx_in = (flags & RADIK_WITHIDXIN) ? iin : nullptr;
+    p.idx_bytes = idx_bytes;
+    p.val_out = vout;
+    p.idx_out = iout;
+    p.err = err_ptr(ws);
+    p.work_counter = ws->state.as<uint32_t>(4);
+    p.gthr = ws->state.as<uint64_t>(kStateHeader);
+    p.task_done = ws->state.as<uint32_t>(kStateHeader + round_up(sizeof(uint64_t) * pl.T, 16));
+    p.cand = ws->cand.as<uint64_t>();
+    p.slot_cnt = ws->slot_cnt.as<uint32_t>();
+    p.sort_scratch = ws->scratch.as<uint64_t>();
+    return p;
+}
+
+int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s) {
+    const Plan& pl = ws->plan;
+    // Reset per-call counters: err stays (sticky until read), work counter,
+    // thresholds and done counters are zeroed.
+    RADIK_CUDA(cudaMemsetAsync(ws->state.as<char>(4), 0,
+                               kStateHeader - 4 + round_up(sizeof(uint64_t) * pl.T, 16) + sizeof(uint32_t) * pl.T, s));
+    FusedKernel fk = pick_fused(pl.threads, pl.vec, (flags & RADIK_WITHSCALE) != 0);
+    fk<<<pl.grid, pl.threads, pl.smem, s>>>(p);
+    RADIK_CUDA(cudaGetLastError());
+    return RADIK_OK;
+}
+
+int run_plain(radik_ws* ws, const FusedParams& fp, uint32_t flags, cudaStream_t s) {
+    const Plan& pl = ws->plan;
+    const int64_t T = pl.T;
+    const uint32_t k = fp.k;
+    const bool scale = (flags & RADIK_WITHSCALE) != 0;
+    PlainParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.data = fp.data;
+    p.tasks = fp.tasks;
+    p.segs = fp.segs;
+    p.nsegs = pl.nsegs;
+    p.ntasks = static_cast<int32_t>(T);
+    p.k = k;
+    p.sp = fp.sp;
+    p.hist = ws->hist.as<uint32_t>();
+    p.st = ws->pstate.as<PlainState>();
+    p.out_stage = ws->stage.as<uint64_t>();
+    p.cand[0] = ws->pcand[0].as<uint64_t>();
+    p.cand[1] = ws->pcand[1].as<uint64_t>();
+    p.err = fp.err;
+    uint32_t* any = ws->state.as<uint32_t>(8);
+    const DeviceInfo di = device_info();
+    const int grid_in = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pl.nsegs, 8LL * di.sms)));
+
+    RADIK_CUDA(cudaMemsetAsync(p.hist, 0, sizeof(uint32_t) * 4096 * T, s));
+    RADIK_CUDA(cudaMemsetAsync(p.st, 0, sizeof(PlainState) * T, s));
+    if (scale) plain_hist_input<256, true><<<grid_in, 256, 0, s>>>(p);
+    else plain_hist_input<256, false><<<grid_in, 256, 0, s>>>(p);
+    plain_select<256><<<static_cast<unsigned>(T), 256, 0, s>>>(p, 0, 12);
+    if (scale) plain_compact_input<256, true><<<grid_in, 256, 0, s>>>(p);
+    else plain_compact_input<256, false><<<grid_in, 256, 0, s>>>(p);
+    RADIK_CUDA(cudaMemsetAsync(any, 0, 4, s));
+    plain_advance<<<static_cast<unsigned>((T + 255) / 256), 256, 0, s>>>(p, any);
+    RADIK_CUDA(cudaGetLastError());
+
+    // Candidate passes over the remaining composite bits; the host reads the
+    // "any task active" flag after each pass (src/algorithm.jl:242-244,
+    // :275-277 read back candidate counts the same way).
+    static const int kSh[5] = {40, 32, 20, 8, 0};
+    static const int kW[5] = {12, 8, 12, 12, 8};
+    int src = 0;
+    for (int ps = 0; ps < 5; ++ps) {
+        uint32_t h_any = 0;
+        RADIK_CUDA(cudaMemcpyAsync(&h_any, any, 4, cudaMemcpyDeviceToHost, s));
+        RADIK_CUDA(cudaStreamSynchronize(s));
+        if (!h_any) break;
+        int64_t maxlen = 0;
+        for (int64_t t = 0; t < T; ++t) maxlen = std::max(maxlen, pl.tasks[t].len);
+        const unsigned gx = static_cast<unsigned>(std::max<int64_t>(
+            1, std::min<int64_t>((maxlen + 255) / 256, std::max<int64_t>(1, 4LL * di.sms / std::max<int64_t>(T, 1)))));
+        for (int64_t t0 = 0; t0 < T; t0 += 65535) {
+            unsigned gy = static_cast<unsigned>(std::min<int64_t>(65535, T - t0));
+            plain_hist_cand<256><<<dim3(gx, gy), 256, 0, s>>>(p, static_cast<int>(t0), src, kSh[ps], kW[ps]);
+        }
+        plain_select<256><<<static_cast<unsigned>(T), 256, 0, s>>>(p, ps + 1, kW[ps]);
+        for (int64_t t0 = 0; t0 < T; t0 += 65535) {
+            unsigned gy = static_cast<unsigned>(std::min<int64_t>(65535, T - t0));
+            plain_compact_cand<256><<<dim3(gx, gy), 256, 0, s>>>(p, static_cast<int>(t0), src, kSh[ps], kW[ps]);
+        }
+        RADIK_CUDA(cudaMemsetAsync(any, 0, 4, s));
+        plain_advance<<<static_cast<unsigned>((T + 255) / 256), 256, 0, s>>>(p, any);
+        RADIK_CUDA(cudaGetLastError());
+        src ^= 1;
+    }
+    const size_t fsmem = std::max<size_t>(sizeof(uint64_t) * kBitonicMax, sizeof(uint32_t) * (8 * 256 + 256));
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(reinterpret_cast<const void*>(plain_finalize<256>),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(fsmem));
+        attr_set = true;
+    }
+    if (T > 0) plain_finalize<256><<<static_cast<unsigned>(T), 256, fsmem, s>>>(p, fp, ws->scratch.as<uint64_t>());
+    RADIK_CUDA(cudaGetLastError());
+    return RADIK_OK;
+}
+
+int finish_sync(radik_ws* ws, cudaStream_t s) {
+    RADIK_CUDA(cudaMemcpyAsync(ws->h_err, err_ptr(ws), 4, cudaMemcpyDeviceToHost, s));
+    RADIK_CUDA(cudaStreamSynchronize(s));
+    if (*ws->h_err) {
+        uint32_t bits = *ws->h_err;
+        cudaMemsetAsync(err_ptr(ws), 0, 4, s);
+        cudaStreamSynchronize(s);
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "device error word 0x%x (capacity=1 bounds=2 timeout=4 internal=8)", bits);
+        return fail((bits & kErrTimeout) ? RADIK_ERR_TIMEOUT : RADIK_ERR_DEVICE, buf);
+    }
+    return RADIK_OK;
+}
+
+int validate_lens(const int64_t* lens, int64_t T, int64_t* maxlen) {
+    *maxlen = 0;
+    for (int64_t t = 0; t < T; ++t) {
+        if (lens[t] < 0) return fail(RADIK_ERR_INVALID, "task_lens must be non-negative");
+        if (lens[t] > INT32_MAX) return fail(RADIK_ERR_INVALID, "a task may hold at most 2^31-1 elements");
+        *maxlen = std::max(*maxlen, lens[t]);
+    }
+    return RADIK_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Exported API
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* radik_version(void) { return "radik-b200 0.1.0 (sm_100a)"; }
+
+const char* radik_last_error(void) { return g_last_error.c_str(); }
+
+const char* radik_status_string(int st) {
+    switch (st) {
+        case RADIK_OK: return "ok";
+        case RADIK_ERR_INVALID: return "invalid argument";
+        case RADIK_ERR_OOM: return "out of memory";
+        case RADIK_ERR_WS_TOO_SMALL: return "workspace too small";
+        case RADIK_ERR_CUDA: return "CUDA error";
+        case RADIK_ERR_DEVICE: return "device-side error";
+        case RADIK_ERR_TIMEOUT: return "device wait timed out";
+        case RADIK_ERR_CAPTURE: return "not allowed during stream capture";
+        default: return "unknown status";
+    }
+}
+
+int radik_ws_create(int64_t n, int64_t num_tasks, int index_bytes, radik_ws** out) {
+    if (!out) return fail(RADIK_ERR_INVALID, "ws pointer is NULL");
+    *out = nullptr;
+    if (n < 0 || num_tasks < 0) return fail(RADIK_ERR_INVALID, "workspace sizes must be non-negative");
+    if (index_bytes != 4 && index_bytes != 8) return fail(RADIK_ERR_INVALID, "workspace integer type must be 4 or 8 bytes");
+    radik_ws* ws = new (std::nothrow) radik_ws();
+    if (!ws) return fail(RADIK_ERR_OOM, "host allocation of the workspace failed");
+    cudaGetDevice(&ws->device);
+    ws->n = n;
+    ws->num_tasks = num_tasks;
+    ws->index_bytes = index_bytes;
+    if (cudaMallocHost(&ws->h_err, sizeof(uint32_t)) != cudaSuccess) {
+        delete ws;
+        return fail(RADIK_ERR_OOM, "pinned allocation failed");
+    }
+    *ws->h_err = 0;
+    const size_t sb = kStateHeader + round_up(sizeof(uint64_t) * std::max<int64_t>(num_tasks, 1), 16) +
+                      sizeof(uint32_t) * std::max<int64_t>(num_tasks, 1);
+    if (ws->state.ensure(sb) != cudaSuccess || cudaMemset(ws->state.p, 0, sb) != cudaSuccess) {
+        cudaFreeHost(ws->h_err);
+        delete ws;
+        return fail(RADIK_ERR_OOM, "device allocation of the workspace failed");
+    }
+    *out = ws;
+    return RADIK_OK;
+}
+
+int radik_ws_destroy(radik_ws* ws) {
+    if (!ws) return RADIK_OK;
+    for (DevBuf* b : {&ws->state, &ws->desc, &ws->cand, &ws->slot_cnt, &ws->scratch, &ws->hist, &ws->pstate,
+                      &ws->stage, &ws->pcand[0], &ws->pcand[1], &ws->io_in, &ws->io_idx, &ws->io_vout, &ws->io_iout})
+        b->release();
+    if (ws->h_err) cudaFreeHost(ws->h_err);
+    delete ws;
+    return RADIK_OK;
+}
+
+int radik_ws_bytes(const radik_ws* ws, size_t* bytes) {
+    if (!ws || !bytes) return fail(RADIK_ERR_INVALID, "NULL argument");
+    size_t b = 0;
+    for (const DevBuf* d : {&ws->state, &ws->desc, &ws->cand, &ws->slot_cnt, &ws->scratch, &ws->hist, &ws->pstate,
+                            &ws->stage, &ws->pcand[0], &ws->pcand[1], &ws->io_in, &ws->io_idx, &ws->io_vout,
+                            &ws->io_iout})
+        b += d->bytes;
+    *bytes = b;
+    return RADIK_OK;
+}
+
+int radik_ws_error(radik_ws* ws, uint32_t* bits) {
+    if (!ws || !bits) return fail(RADIK_ERR_INVALID, "NULL argument");
+    RADIK_CUDA(cudaMemcpyAsync(ws->h_err, err_ptr(ws), 4, cudaMemcpyDeviceToHost, ws->last_stream));
+    RADIK_CUDA(cudaStreamSynchronize(ws->last_stream));
+    *bits = *ws->h_err;
+    RADIK_CUDA(cudaMemsetAsync(err_ptr(ws), 0, 4, ws->last_stream));
+    RADIK_CUDA(cudaStreamSynchronize(ws->last_stream));
+    return RADIK_OK;
+}
+
+int radik_ws_prepare(radik_ws* ws, const int64_t* h_task_lens, int64_t num_tasks, int64_t k, uint32_t flags,
+                     int idx_bytes) {
+    if (!ws || (!h_task_lens && num_tasks > 0)) return fail(RADIK_ERR_INVALID, "NULL argument");
+    if (k < 0) return fail(RADIK_ERR_INVALID, "k must be non-negative");
+    if (idx_bytes != 4 && idx_bytes != 8) return fail(RADIK_ERR_INVALID, "index width must be 4 or 8 bytes");
+    int64_t maxlen = 0;
+    int rc = validate_lens(h_task_lens, num_tasks, &maxlen);
+    if (rc) return rc;
+    if (maxlen > ws->n || num_tasks > ws->num_tasks)
+        return fail(RADIK_ERR_WS_TOO_SMALL, "workspace requires n >= max(task_lens) and num_tasks <= its num_tasks");
+    return build_plan(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
+}
+
+int radik_topk_radix_select(float* d_val_out, void* d_idx_out, int idx_bytes, radik_ws* ws, const float* d_val_in,
+                            const void* d_idx_in, const int64_t* h_task_lens, int64_t num_tasks, int64_t k,
+                            uint32_t flags, void* stream) {
+    if (!ws) return fail(RADIK_ERR_INVALID, "workspace is NULL");
+    if (num_tasks < 0 || k < 0) return fail(RADIK_ERR_INVALID, "num_tasks and k must be non-negative");
+    if (idx_bytes != 4 && idx_bytes != 8) return fail(RADIK_ERR_INVALID, "index width must be 4 or 8 bytes");
+    if (k > INT32_MAX) return fail(RADIK_ERR_INVALID, "k must fit in 32 bits");
+    if ((flags & RADIK_WITHIDXIN) && !d_idx_in) return fail(RADIK_ERR_INVALID, "WITHIDXIN needs idx_in");
+    if (num_tasks == 0 || k == 0) return RADIK_OK;
+    if (!d_val_out || !d_idx_out || !h_task_lens) return fail(RADIK_ERR_INVALID, "NULL output or task_lens");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    ws->last_stream = s;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cap);
+    int64_t maxlen = 0;
+    int rc = validate_lens(h_task_lens, num_tasks, &maxlen);
+    if (rc) return rc;
+    if (maxlen > ws->n || num_tasks > ws->num_tasks)
+        return fail(RADIK_ERR_WS_TOO_SMALL, "workspace requires n >= max(task_lens) and num_tasks <= its num_tasks");
+    if (maxlen > 0 && !d_val_in) return fail(RADIK_ERR_INVALID, "val_in is NULL");
+    if ((reinterpret_cast<uintptr_t>(d_val_in) & 3) || (reinterpret_cast<uintptr_t>(d_val_out) & 3) ||
+        (reinterpret_cast<uintptr_t>(d_idx_out) & (idx_bytes - 1)) ||
+        ((flags & RADIK_WITHIDXIN) && (reinterpret_cast<uintptr_t>(d_idx_in) & (idx_bytes - 1))))
+        return fail(RADIK_ERR_INVALID, "device arrays must be aligned to their element size");
+    {
+        PlanKey key;
+        key.lens.assign(h_task_lens, h_task_lens + num_tasks);
+        key.k = k;
+        key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
+        key.idx_bytes = idx_bytes;
+        if (!(ws->plan.valid && ws->plan.key == key)) {
+            if (cap != cudaStreamCaptureStatusNone)
+                return fail(RADIK_ERR_CAPTURE, "no prepared plan for this shape: call radik_ws_prepare before capture");
+            rc = build_plan(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
+            if (rc) return rc;
+        }
+    }
+    FusedParams p = fused_params(ws, d_val_out, d_idx_out, idx_bytes, d_val_in, d_idx_in, k, flags);
+    if (ws->plan.fused) {
+        rc = run_fused(ws, p, flags, s);
+    } else {
+        if (cap != cudaStreamCaptureStatusNone)
+            return fail(RADIK_ERR_CAPTURE, "the multi-pass path synchronises with the host and cannot be captured");
+        rc = run_plain(ws, p, flags, s);
+    }
+    if (rc) return rc;
+    if (flags & RADIK_ASYNC) return RADIK_OK;
+    return finish_sync(ws, s);
+}
+
+int radik_topk(float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_data, int64_t data_len,
+               const void* d_indices, int64_t indices_len, const int64_t* h_task_lens, int64_t num_tasks, int64_t k,
+               int largest, int rev, void* stream) {
+    if (num_tasks < 0 || k < 0) return fail(RADIK_ERR_INVALID, "num_tasks and k must be non-negative");
+    int64_t maxlen = 0, total = 0;
+    int rc = validate_lens(h_task_lens, num_tasks, &maxlen);
+    if (rc) return rc;
+    for (int64_t t = 0; t < num_tasks; ++t) total += h_task_lens[t];
+    if (total > data_len) return fail(RADIK_ERR_INVALID, "sum(task_lens) exceeds the data length");
+    // src/algorithm.jl:506-510
+    if (d_indices && indices_len > 0 && indices_len != data_len) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "indices length must equal data length. Got %lld vs %lld",
+                      static_cast<long long>(indices_len), static_cast<long long>(data_len));
+        return fail(RADIK_ERR_INVALID, buf);
+    }
+    radik_ws* ws = nullptr;
+    rc = radik_ws_create(maxlen, num_tasks, 4, &ws);  // fresh workspace per call (:503)
+    if (rc) return rc;
+    uint32_t flags = (largest ? RADIK_LARGEST : 0u) | (rev ? 0u : RADIK_ASCEND) | RADIK_WITHPACKING;
+    if (d_indices && indices_len > 0) flags |= RADIK_WITHIDXIN;
+    rc = radik_topk_radix_select(d_val_out, d_idx_out, idx_bytes, ws, d_data, d_indices, h_task_lens, num_tasks, k,
+                                 flags, stream);
+    std::string keep = g_last_error;
+    radik_ws_destroy(ws);
+    g_last_error = keep;
+    return rc;
+}
+
+int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const float* h_data, int64_t data_len,
+                    const void* h_indices, int64_t indices_len, const int64_t* h_task_lens, int64_t num_tasks,
+                    int64_t k, int largest, int rev, radik_ws* ws, void* stream) {
+    if (!ws) return fail(RADIK_ERR_INVALID, "workspace is NULL");
+    if (idx_bytes != 4 && idx_bytes != 8) return fail(RADIK_ERR_INVALID, "index width must be 4 or 8 bytes");
+    if (h_indices && indices_len > 0 && indices_len != data_len) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "indices length must equal data length. Got %lld vs %lld",
+                      static_cast<long long>(indices_len), static_cast<long long>(data_len));
+        return fail(RADIK_ERR_INVALID, buf);
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool with_idx = h_indices && indices_len > 0;
+    const size_t out_n = static_cast<size_t>(num_tasks) * static_cast<size_t>(k);
+    cudaError_t e = ws->io_in.ensure(sizeof(float) * static_cast<size_t>(data_len));
+    if (e == cudaSuccess && with_idx) e = ws->io_idx.ensure(static_cast<size_t>(idx_bytes) * data_len);
+    if (e == cudaSuccess) e = ws->io_vout.ensure(sizeof(float) * out_n);
+    if (e == cudaSuccess) e = ws->io_iout.ensure(static_cast<size_t>(idx_bytes) * out_n);
+    if (e != cudaSuccess) return fail(RADIK_ERR_OOM, std::string("io buffers: ") + cudaGetErrorString(e));
+    RADIK_CUDA(cudaMemcpyAsync(ws->io_in.p, h_data, sizeof(float) * data_len, cudaMemcpyHostToDevice, s));
+    if (with_idx)
+        RADIK_CUDA(cudaMemcpyAsync(ws->io_idx.p, h_indices, static_cast<size_t>(idx_bytes) * data_len,
+                                   cudaMemcpyHostToDevice, s));
+    uint32_t flags = (largest ? RADIK_LARGEST : 0u) | (rev ? 0u : RADIK_ASCEND) | RADIK_ASYNC;
+    if (with_idx) flags |= RADIK_WITHIDXIN;
+    int rc = radik_topk_radix_select(ws->io_vout.as<float>(), ws->io_iout.p, idx_bytes, ws, ws->io_in.as<float>(),
+                                     with_idx ? ws->io_idx.p : nullptr, h_task_lens, num_tasks, k, flags, stream);
+    if (rc) return rc;
+    if (out_n) {
+        RADIK_CUDA(cudaMemcpyAsync(h_val_out, ws->io_vout.p, sizeof(float) * out_n, cudaMemcpyDeviceToHost, s));
+        RADIK_CUDA(cudaMemcpyAsync(h_idx_out, ws->io_iout.p, static_cast<size_t>(idx_bytes) * out_n,
+                                   cudaMemcpyDeviceToHost, s));
+    }
+    return finish_sync(ws, s);
+}
+
+// ---- stage entry points ----------------------------------------------------
+
+namespace {
+int upload_stage_tasks(const int64_t* lens, int64_t T, DevBuf& buf, cudaStream_t s, int64_t stride = -1) {
+    std::vector<StageTask> v(T);
+    int64_t off = 0;
+    for (int64_t t = 0; t < T; ++t) {
+        v[t].start = stride >= 0 ? t * stride : off;
+        v[t].len = lens[t];
+        off += lens[t];
+    }
+    if (buf.ensure(sizeof(StageTask) * std::max<int64_t>(T, 1)) != cudaSuccess) return fail(RADIK_ERR_OOM, "stage tasks");
+    RADIK_CUDA(cudaMemcpyAsync(buf.p, v.data(), sizeof(StageTask) * T, cudaMemcpyHostToDevice, s));
+    RADIK_CUDA(cudaStreamSynchronize(s));
+    return RADIK_OK;
+}
+
+int check_bits(int left, int right, int* hist_len) {
+    if (left < 0 || left > 31 || right < 20 || right > 31)
+        return fail(RADIK_ERR_INVALID, "LEFT must be in [0,31] and RIGHT in [20,31] (at most 4096 bins)");
+    *hist_len = 1 << (32 - right);
+    return RADIK_OK;
+}
+}  // namespace
+
+int radik_count_bin_ex(int32_t* d_hist, const float* d_data, const int64_t* h_task_lens, int64_t num_tasks, int left,
+                       int right, int withscale, int largest, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int hl = 0;
+    int rc = check_bits(left, right, &hl);
+    if (rc) return rc;
+    if (num_tasks <= 0) return RADIK_OK;
+    DevBuf tb;
+    rc = upload_stage_tasks(h_task_lens, num_tasks, tb, s);
+    if (rc) { tb.release(); return rc; }
+    RADIK_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(int32_t) * hl * num_tasks, s));
+    const DeviceInfo di = device_info();
+    dim3 grid(static_cast<unsigned>(std::max(1, 2 * di.sms / static_cast<int>(std::min<int64_t>(num_tasks, 2 * di.sms)))),
+              static_cast<unsigned>(std::min<int64_t>(num_tasks, 65535)));
+    stage_count_bin_ex<<<grid, 256, sizeof(int32_t) * hl, s>>>(d_hist, d_data, tb.as<StageTask>(), num_tasks, left,
+                                                                 right, hl, withscale, largest);
+    cudaError_t e = cudaStreamSynchronize(s);
+    tb.release();
+    if (e != cudaSuccess) return fail(RADIK_ERR_CUDA, cudaGetErrorString(e));
+    return RADIK_OK;
+}
+
+int radik_count_bin(int32_t* d_hist, const float* d_data, const int64_t* h_task_lens, int64_t stride,
+                    int64_t num_tasks, int left, int right, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int hl = 0;
+    int rc = check_bits(left, right, &hl);
+    if (rc) return rc;
+    if (num_tasks <= 0) return RADIK_OK;
+    for (int64_t t = 0; t < num_tasks; ++t)
+        if (h_task_lens[t] > stride) return fail(RADIK_ERR_INVALID, "task_lens must not exceed stride");
+    DevBuf tb;
+    rc = upload_stage_tasks(h_task_lens, num_tasks, tb, s, stride);
+    if (rc) { tb.release(); return rc; }
+    RADIK_CUDA(cudaMemsetAsync(d_hist, 0, sizeof(int32_t) * hl * num_tasks, s));
+    dim3 grid(8, static_cast<unsigned>(std::min<int64_t>(num_tasks, 65535)));
+    stage_count_bin<<<grid, 256, sizeof(int32_t) * hl, s>>>(d_hist, d_data, tb.as<StageTask>(), stride, num_tasks,
+                                                              left, right, hl);
+    cudaError_t e = cudaStreamSynchronize(s);
+    tb.release();
+    if (e != cudaSuccess) return fail(RADIK_ERR_CUDA, cudaGetErrorString(e));
+    return RADIK_OK;
+}
+
+int radik_select_bin(int32_t* d_bin_ids, int32_t* d_k_values, int32_t* d_counts, const int32_t* d_hist,
+                     int64_t num_tasks, int64_t hist_len, int largest, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (hist_len <= 0 || hist_len > (1 << 20)) return fail(RADIK_ERR_INVALID, "hist_len out of range");
+    if (num_tasks <= 0) return RADIK_OK;
+    stage_select_bin<256><<<static_cast<unsigned>(num_tasks), 256, 0, s>>>(d_bin_ids, d_k_values, d_counts, d_hist,
+                                                                           hist_len, largest);
+    RADIK_CUDA(cudaGetLastError());
+    RADIK_CUDA(cudaStreamSynchronize(s));
+    return RADIK_OK;
+}
+
+int radik_filter(float* d_val_out, void* d_idx_out, int idx_bytes, int32_t* d_counts, int32_t* d_boundary,
+                 const float* d_data, const void* d_idx_in, const float* d_kth, const int64_t* h_task_lens,
+                 int64_t num_tasks, int64_t k, int withscale, int largest, void* stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (idx_bytes != 4 && idx_bytes != 8) return fail(RADIK_ERR_INVALID, "index width must be 4 or 8 bytes");
+    if (num_tasks <= 0) return RADIK_OK;
+    DevBuf tb, eb;
+    int rc = upload_stage_tasks(h_task_lens, num_tasks, tb, s);
+    if (rc) { tb.release(); return rc; }
+    if (eb.ensure(4) != cudaSuccess) { tb.release(); return fail(RADIK_ERR_OOM, "error word"); }
+    cudaMemsetAsync(eb.p, 0, 4, s);
+    RADIK_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(int32_t) * num_tasks, s));
+    dim3 grid(16, static_cast<unsigned>(std::min<int64_t>(num_tasks, 65535)));
+    stage_filter<<<grid, 256, 0, s>>>(d_val_out, d_idx_out, idx_bytes, d_counts, d_boundary, d_data, d_idx_in, d_kth,
+                                      tb.as<StageTask>(), num_tasks, k, withscale, largest, eb.as<uint32_t>());
+    uint32_t h = 0;
+    cudaMemcpyAsync(&h, eb.p, 4, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    tb.release();
+    eb.release();
+    if (e != cudaSuccess) return fail(RADIK_ERR_CUDA, cudaGetErrorString(e));
+    if (h) return fail(RADIK_ERR_DEVICE, "filter emitted more than k elements for a task (output bounded)");
+    return RADIK_OK;
+}
+
+}  // extern "C"
