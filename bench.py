@@ -1,0 +1,432 @@
+"""Benchmark of the B200 exact Float32 radix top-k (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config uniform_batch|adversarial_single|uneven_batch]
+
+A step is one batched top-k over the configuration's synthetic input (seeded,
+shapes and distributions of the workload; no dataset exists):
+  uniform_batch       1024 tasks x 65,536 Float32 U(0,1) (seed 1), k=256,
+                      largest, one topk_radix_select! into (1024, 256) outputs
+  adversarial_single  one task of 2^28 Float32 (seed 2): 50% from 1024 distinct
+                      N(0,1) values, 40% in [1, 1+2^-10), 10% N(0,100^2);
+                      k=4096, largest=false, rev=true
+  uneven_batch        4096 tasks, lengths lognormal(median 20,000, sigma 1.5)
+                      clamped to [1, 4,194,304] (seed 3), N(0,1), custom Int32
+                      indices (a permutation), k=64, largest
+`value` is elements/s with the inputs already in HBM (timed with CUDA events
+on the launching stream, max over ranks); `e2e` is the same metric through the
+host-buffer public entry point (pinned host input copied in and results copied
+back every step).  Multi-GPU runs are independent replicas of the per-GPU
+batch (tasks are independent; no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+L2_BYTES = 126 * 1024 * 1024
+
+
+def load_package():
+    import importlib.util
+    if "radik_b200" in sys.modules:
+        return sys.modules["radik_b200"]
+    pkg = ROOT / "radik.jl_b200"
+    spec = importlib.util.spec_from_file_location("radik_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["radik_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_oracle():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle  # the CPU baseline only
+    sys.path.pop(0)
+    return oracle
+
+
+# ---------------------------------------------------------------------------
+# Workloads
+# ---------------------------------------------------------------------------
+CONFIGS = {
+    "uniform_batch": dict(k=256, largest=True, rev=False, custom_idx=False),
+    "adversarial_single": dict(k=4096, largest=False, rev=True, custom_idx=False),
+    "uneven_batch": dict(k=64, largest=True, rev=False, custom_idx=True),
+}
+
+
+def task_lens_of(name: str) -> list[int]:
+    if name == "uniform_batch":
+        return [65536] * 1024
+    if name == "adversarial_single":
+        return [1 << 28]
+    rng = np.random.default_rng(3)
+    v = np.clip(np.round(rng.lognormal(np.log(20000), 1.5, size=4096)), 1, 4_194_304)
+    return [int(x) for x in v]
+
+
+def make_input_np(name: str, N: int, seed_offset: int = 0) -> np.ndarray:
+    if name == "uniform_batch":
+        return np.random.default_rng(1 + seed_offset).random(N, dtype=np.float32)
+    if name == "adversarial_single":
+        rng = np.random.default_rng(2 + seed_offset)
+        pool = rng.standard_normal(1024).astype(np.float32)
+        u = rng.random(N, dtype=np.float32)
+        out = np.empty(N, np.float32)
+        a = u < 0.5
+        b = (u >= 0.5) & (u < 0.9)
+        c = u >= 0.9
+        out[a] = pool[rng.integers(0, 1024, size=int(a.sum()))]
+        out[b] = (1.0 + rng.random(int(b.sum()), dtype=np.float32) * np.float32(2.0 ** -10)).astype(np.float32)
+        out[c] = (rng.standard_normal(int(c.sum())).astype(np.float32) * np.float32(100.0))
+        return out
+    return np.random.default_rng(3 + seed_offset).standard_normal(N).astype(np.float32)
+
+
+def make_input_dev(torch, name: str, N: int, seed: int):
+    """Same distributions generated on the device (fast for 2^28 elements)."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    if name == "uniform_batch":
+        return torch.rand(N, device="cuda", generator=g)
+    if name == "adversarial_single":
+        pool = torch.randn(1024, device="cuda", generator=g)
+        u = torch.rand(N, device="cuda", generator=g)
+        a = pool[torch.randint(0, 1024, (N,), device="cuda", generator=g)]
+        b = 1.0 + torch.rand(N, device="cuda", generator=g) * (2.0 ** -10)
+        c = torch.randn(N, device="cuda", generator=g) * 100.0
+        return torch.where(u < 0.5, a, torch.where(u < 0.9, b, c)).contiguous()
+    return torch.randn(N, device="cuda", generator=g)
+
+
+# ---------------------------------------------------------------------------
+# Clocks (sampled during the timed region)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic(config: str):
+    p = ROOT / "profiles" / "traffic.json"
+    try:
+        d = json.loads(p.read_text())
+        return d.get(config)
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+# Arms
+# ---------------------------------------------------------------------------
+def run_reference(args, rank: int, world: int):
+    """CPU arm: the oracle port of the reference algorithm on all host
+    threads, over a bounded sample of the same workload per step."""
+    if rank != 0:
+        return
+    oracle = load_oracle()
+    cfg = CONFIGS[args.config]
+    lens = task_lens_of(args.config)
+    threads = oracle.max_threads()
+    if args.config == "uniform_batch":
+        sample_lens = lens[:64]
+        sample = f"64 of the 1024 tasks ({64 * 65536} elements) per step"
+    elif args.config == "adversarial_single":
+        sample_lens = [1 << 22]
+        sample = "a 2^22-element prefix task of the same mixture per step"
+    else:
+        sample_lens = lens[:256]
+        sample = "the first 256 of the 4096 tasks per step"
+    N = int(sum(sample_lens))
+    x = make_input_np(args.config, N)
+    ind = np.arange(N, dtype=np.int32) if cfg["custom_idx"] else None
+    for _ in range(args.warmup):
+        oracle.topk(x, sample_lens, cfg["k"], largest=cfg["largest"], rev=cfg["rev"], indices=ind, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.topk(x, sample_lens, cfg["k"], largest=cfg["largest"], rev=cfg["rev"], indices=ind, threads=threads)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    value = N / dt
+    line = {
+        "impl": "reference", "metric": "elements/s", "value": value, "unit": "elements/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.config, "task_lens": "see bench.py", "k": cfg["k"],
+                   "largest": cfg["largest"], "rev": cfg["rev"]},
+        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "RadiK.jl is Julia; no Julia toolchain on this machine, so the reference arm is the C "
+                "restatement of its algorithm (oracle/) on the host cores",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_quick(args) -> dict:
+    """Bounded CPU sample (oracle port, all host threads) for the JSON line."""
+    oracle = load_oracle()
+    cfg = CONFIGS[args.config]
+    lens = task_lens_of(args.config)
+    if args.config == "uniform_batch":
+        sl, sample = lens[:64], "64 of the 1024 tasks, 3 repetitions"
+    elif args.config == "adversarial_single":
+        sl, sample = [1 << 22], "one 2^22-element task of the same mixture, 3 repetitions"
+    else:
+        sl, sample = lens[:256], "first 256 of the 4096 tasks, 3 repetitions"
+    N = int(sum(sl))
+    x = make_input_np(args.config, N)
+    threads = oracle.max_threads()
+    oracle.topk(x, sl, cfg["k"], largest=cfg["largest"], rev=cfg["rev"], threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        oracle.topk(x, sl, cfg["k"], largest=cfg["largest"], rev=cfg["rev"], threads=threads)
+    dt = (time.perf_counter() - t0) / 3
+    return {"value": N / dt, "unit": "elements/s", "cores": threads, "kind": "port", "sample": sample}
+
+
+def run_ours(args, rank: int, world: int, dist):
+    import torch
+    radik = load_package()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    cfg = CONFIGS[args.config]
+    lens = task_lens_of(args.config)
+    T, k, N = len(lens), cfg["k"], int(sum(lens))
+    # Inputs: enough rotating copies that the bytes touched between two reads
+    # of the same buffer exceed the L2 several times.
+    nbuf = max(2, int(np.ceil(3 * L2_BYTES / (4 * N))) + 1)
+    xs = [make_input_dev(torch, args.config, N, seed=1000 * rank + i + 1) for i in range(nbuf)]
+    ind = None
+    if cfg["custom_idx"]:
+        g = torch.Generator(device="cuda")
+        g.manual_seed(7 + rank)
+        ind = torch.randperm(N, device="cuda", generator=g).to(torch.int32)
+    vo = torch.empty((T, k), dtype=torch.float32, device="cuda")
+    io = torch.empty((T, k), dtype=torch.int32, device="cuda")
+    ws = radik.RadiKWorkspace("cuda", max(lens), T)
+    ws.prepare(lens, k, largest=cfg["largest"], ascend=not cfg["rev"], withidxin=ind is not None)
+    stream = torch.cuda.current_stream()
+
+    def step(i):
+        radik.topk_radix_select_(vo, io, ws, xs[i % nbuf], ind, lens, k, cfg["largest"], not cfg["rev"],
+                                 False, ind is not None, sync=False, stream=stream)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if ws.error_bits():
+        raise RuntimeError("device error during warm-up")
+
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    per = []
+    ev0.record(stream)
+    for i in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step(i)
+        b.record(stream)
+        per.append((a, b))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = ev0.elapsed_time(ev1)
+    launch_ms = [a.elapsed_time(b) for a, b in per]
+    if ws.error_bits():
+        raise RuntimeError("device error during the timed steps")
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = N * world / (ms_per_step * 1e-3)
+
+    # Roofline of the dominant kernel (the fused single-read kernel is the
+    # only kernel of a step): algorithmic bytes = one read of the input +
+    # the (value, index) outputs (+ the gathered custom indices).
+    idx_b = 4
+    alg_bytes = 4 * N + (4 + idx_b) * T * k + (idx_b * T * k if ind is not None else 0)
+    avg_launch_s = statistics.mean(launch_ms) * 1e-3
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg_bytes / avg_launch_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": profile_traffic(args.config), "peak_source": peak_kind,
+                "kernel": "fused_topk_kernel", "algorithmic_bytes_per_launch": alg_bytes}
+
+    # End to end through the host-buffer entry point (pinned host memory).
+    e2e = None
+    if not args.no_e2e:
+        hx = torch.empty(N, dtype=torch.float32, pin_memory=True)
+        hx.copy_(xs[0].cpu())
+        hx_np = hx.numpy()
+        hv = torch.empty((T, k), dtype=torch.float32, pin_memory=True).numpy()
+        hi = torch.empty((T, k), dtype=torch.int32, pin_memory=True).numpy()
+        hind = None
+        if ind is not None:
+            hind_t = torch.empty(N, dtype=torch.int32, pin_memory=True)
+            hind_t.copy_(ind.cpu())
+            hind = hind_t.numpy()
+        ws_e = radik.RadiKWorkspace("cuda", max(lens), T)
+        e_steps = max(2, min(args.steps, 10))
+        for _ in range(2):
+            radik.topk_host(hx_np, lens, k, indices=hind, largest=cfg["largest"], rev=cfg["rev"], ws=ws_e,
+                            out=(hv, hi))
+        barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(e_steps):
+            radik.topk_host(hx_np, lens, k, indices=hind, largest=cfg["largest"], rev=cfg["rev"], ws=ws_e,
+                            out=(hv, hi), stream=stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        e_ms = torch.tensor([a.elapsed_time(b) / e_steps], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
+        h2d = 4 * N + (4 * N if hind is not None else 0)
+        e2e = {"value": N * world / (float(e_ms.item()) * 1e-3), "unit": "elements/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": (4 + idx_b) * T * k,
+               "steps": e_steps, "ms_per_step": float(e_ms.item())}
+        ws_e.close()
+
+    # Plain per-call path (reference-shaped multi-pass, fresh workspace and a
+    # synchronisation per call) for the same batch, a few calls.
+    plain = None
+    if not args.no_plain and rank == 0:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ncall = 3
+        for i in range(ncall):
+            radik.topk_(vo, io, xs[i % nbuf], lens, k, indices=ind, largest=cfg["largest"], rev=cfg["rev"],
+                        plain=True)
+        torch.cuda.synchronize()
+        pdt = (time.perf_counter() - t0) / ncall
+        plain = {"value": N / pdt, "unit": "elements/s", "ms_per_call": pdt * 1e3,
+                 "path": "multi-pass per call (fresh workspace, host syncs)"}
+
+    cpu = cpu_baseline_quick(args) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    if rank == 0:
+        line = {
+            "metric": "elements/s", "value": value, "unit": "elements/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.config, "tasks": T, "elements": N, "k": k, "largest": cfg["largest"],
+                       "rev": cfg["rev"], "custom_indices": ind is not None,
+                       "l2": f"inputs larger than L2: {nbuf} rotating input buffers of {4 * N} bytes",
+                       "parallelism": f"replicas x{world} (independent tasks, no collective)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": args.steps, "plain_per_call": plain,
+        }
+        print(json.dumps(line), flush=True)
+    ws.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="uniform_batch", choices=sorted(CONFIGS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,6 +1,7 @@
 // api.cu -- C ABI of the engine (include/radik.h): workspace, launch plans,
 // the fused single-read path, the multi-pass path and the stage entry points.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -12,6 +13,7 @@
 #include "../../include/radik.h"
 #include "fused.cuh"
 #include "general.cuh"
+#include "sample.cuh"
 #include "stages.cuh"
 
 using namespace radik;
@@ -76,16 +78,28 @@ size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // Fused kernel dispatch
 // ---------------------------------------------------------------------------
 using FusedKernel = void (*)(FusedParams);
+constexpr int kStages = 4;  // TMA ring depth of the fused kernel
 
 template <int T, int V, bool S>
-FusedKernel fused_ptr() { return fused_topk_kernel<T, V, S>; }
+FusedKernel fused_ptr() { return fused_topk_kernel<T, V, kStages, S>; }
 
 FusedKernel pick_fused(int threads, int vec, bool scale) {
     if (threads == 256 && vec == 8) return scale ? fused_ptr<256, 8, true>() : fused_ptr<256, 8, false>();
     if (threads == 256 && vec == 16) return scale ? fused_ptr<256, 16, true>() : fused_ptr<256, 16, false>();
     if (threads == 512 && vec == 8) return scale ? fused_ptr<512, 8, true>() : fused_ptr<512, 8, false>();
-    if (threads == 512 && vec == 16) return scale ? fused_ptr<512, 16, true>() : fused_ptr<512, 16, false>();
     return nullptr;
+}
+
+// Dynamic shared memory of the fused kernel: TMA ring, candidate buffer,
+// one mbarrier per ring stage.
+size_t fused_smem(uint32_t cap, int threads, int vec) {
+    return static_cast<size_t>(kStages) * threads * vec * sizeof(float) + static_cast<size_t>(cap) * 8 + kStages * 8;
+}
+
+using SampleKernel = void (*)(FusedParams, const SampleJob*, uint64_t*, uint32_t*);
+
+SampleKernel pick_sample(bool scale) {
+    return scale ? sample_threshold_kernel<256, true> : sample_threshold_kernel<256, false>;
 }
 
 int env_int(const char* name, int dflt) {
@@ -116,10 +130,12 @@ struct Plan {
     uint32_t cap = 0;
     int grid = 0;
     size_t smem = 0;
-    int64_t T = 0, N = 0, slots = 0;
+    int64_t T = 0, N = 0, cand_entries = 0, sample_entries = 0;
     int32_t nsegs = 0;
+    size_t tasks_off = 0, segs_off = 0, jobs_off = 0;
     std::vector<FusedTask> tasks;
     std::vector<FusedSeg> segs;
+    std::vector<SampleJob> jobs;
 };
 
 struct radik_ws {
@@ -129,10 +145,10 @@ struct radik_ws {
     int index_bytes = 4;
     cudaStream_t last_stream = nullptr;
     uint32_t* h_err = nullptr;  // pinned
-    DevBuf state;     // [err, work_counter, any, pad] + gthr[T] + task_done[T]
-    DevBuf desc;      // tasks + segs of the plan
-    DevBuf cand;      // fused: slots * k composites
-    DevBuf slot_cnt;  // fused: slots
+    DevBuf state;     // StateLayout: per-call counters and thresholds
+    DevBuf desc;      // tasks + segs + sample jobs of the plan
+    DevBuf cand;      // fused: candidate regions of multi-segment tasks
+    DevBuf samples;   // fused: sampled composites
     DevBuf scratch;   // sort scratch
     DevBuf hist;      // plain: [T][4096]
     DevBuf pstate;    // plain: [T] PlainState
@@ -144,9 +160,40 @@ struct radik_ws {
 
 namespace {
 
-constexpr size_t kStateHeader = 16;
+// Device state of one workspace.  The header holds the sticky error word and
+// the work counters; everything after `err` is zeroed before every call.
+struct StateLayout {
+    static constexpr size_t kErr = 0, kWork = 4, kWorkRetry = 8, kAny = 12, kHeader = 16;
+    size_t gthr, gthr_r, done, done_r, cnt, cnt_r, fail, sdone, bytes;
+    explicit StateLayout(int64_t T) {
+        const size_t t8 = round_up(sizeof(uint64_t) * static_cast<size_t>(std::max<int64_t>(T, 1)), 16);
+        const size_t t4 = round_up(sizeof(uint32_t) * static_cast<size_t>(std::max<int64_t>(T, 1)), 16);
+        gthr = kHeader;
+        gthr_r = gthr + t8;
+        done = gthr_r + t8;
+        done_r = done + t4;
+        cnt = done_r + t4;
+        cnt_r = cnt + t4;
+        fail = cnt_r + t4;
+        sdone = fail + t4;
+        bytes = sdone + t4;
+    }
+};
 
-uint32_t* err_ptr(radik_ws* ws) { return ws->state.as<uint32_t>(0); }
+uint32_t* err_ptr(radik_ws* ws) { return ws->state.as<uint32_t>(StateLayout::kErr); }
+
+// Shared-buffer capacity of the fused kernel: k entries, one tile of
+// appends, and headroom so that a mid-stream shrink frees room for many
+// tiles of candidates.
+size_t fused_cap(size_t k, size_t tile, int threads) {
+    size_t headroom = std::max<size_t>({k / 2, tile, 1024});
+    size_t cap = k + tile + 8 + headroom;
+    size_t p2 = 1;
+    while (p2 < std::min<size_t>(k, kBitonicMax)) p2 <<= 1;
+    cap = std::max(cap, p2);
+    cap = std::max(cap, k + (static_cast<size_t>(threads) / 32 * 256 + 256) / 2 + 8);
+    return round_up(cap, 64);
+}
 
 // Build the launch plan for a batch shape (host only).
 int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes) {
@@ -165,24 +212,18 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     np.N = 0;
     for (int64_t t = 0; t < T; ++t) np.N += lens[t];
 
-    // Fused configuration: the shared buffer must hold k + one tile.
+    // Fused configuration.  The shared buffer holds k + one tile + headroom;
+    // when that does not fit in shared memory the multi-pass path runs.
     np.threads = env_int("RADIK_THREADS", 256);
-    int64_t avg = T > 0 ? np.N / T : 0;
-    np.vec = env_int("RADIK_VEC", (avg >= (1 << 16)) ? 16 : 8);
+    np.vec = env_int("RADIK_VEC", 8);
     const bool scale = (flags & RADIK_WITHSCALE) != 0;
     FusedKernel fk = pick_fused(np.threads, np.vec, scale);
     if (!fk) return fail(RADIK_ERR_INVALID, "unsupported RADIK_THREADS/RADIK_VEC combination");
     const size_t tile = static_cast<size_t>(np.threads) * np.vec;
-    size_t kk = static_cast<size_t>(k);
-    size_t cap = kk + tile + 8;
-    size_t p2 = 1;
-    while (p2 < std::min<size_t>(kk, kBitonicMax)) p2 <<= 1;
-    cap = std::max(cap, p2);
-    cap = std::max(cap, kk + (static_cast<size_t>(np.threads) / 32 * 256 + 256) / 2 + 8);
-    cap = round_up(cap, 64);
-    np.cap = static_cast<uint32_t>(cap);
-    np.smem = cap * sizeof(uint64_t);
-    np.fused = (flags & RADIK_PLAIN) == 0 && np.smem <= static_cast<size_t>(di.max_smem_optin) - 2048;
+    const size_t kk = static_cast<size_t>(k);
+    np.cap = static_cast<uint32_t>(fused_cap(kk, tile, np.threads));
+    np.smem = fused_smem(np.cap, np.threads, np.vec);
+    np.fused = (flags & RADIK_PLAIN) == 0 && np.smem <= static_cast<size_t>(di.max_smem_optin) - 4096;
 
     int occ = 1;
     if (np.fused) {
@@ -198,8 +239,7 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     const int64_t resident = static_cast<int64_t>(occ) * di.sms;
 
     // Segments: tasks longer than seg_len are split (the last segment of a
-    // task may be shorter); segment boundaries stay 16-byte aligned relative
-    // to the task start.
+    // task may be shorter).
     int64_t seg_len = env_int("RADIK_SEG", 0);
     if (seg_len <= 0) {
         int64_t target = np.N / std::max<int64_t>(1, 3 * resident);
@@ -209,26 +249,60 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     if (!np.fused) seg_len = std::max<int64_t>(seg_len, 1 << 20);
     np.tasks.resize(T);
     np.segs.clear();
-    np.slots = 0;
+    np.jobs.clear();
+    np.cand_entries = 0;
+    np.sample_entries = 0;
     int64_t off = 0;
+    const uint32_t tflags = ((flags & RADIK_LARGEST) ? kTaskLargest : 0u) | ((flags & RADIK_ASCEND) ? kTaskAscend : 0u);
+    const bool allow_sample = env_int("RADIK_SAMPLE", 1) != 0;
     for (int64_t t = 0; t < T; ++t) {
         FusedTask& td = np.tasks[t];
         td.start = off;
         td.len = lens[t];
+        td.k = static_cast<uint32_t>(k);
+        td.flags = tflags;
+        td.pad_ = 0;
         int64_t nseg = 1;
         if (np.fused && td.len > seg_len && td.len > k) nseg = (td.len + seg_len - 1) / seg_len;
         if (!np.fused) nseg = std::max<int64_t>(1, (td.len + seg_len - 1) / seg_len);
         td.nseg = static_cast<int32_t>(nseg);
-        td.slot0 = (np.fused && nseg > 1) ? np.slots : -1;
-        if (np.fused && nseg > 1) np.slots += nseg;
+        td.cbase = -1;
+        if (np.fused && nseg > 1) {
+            td.cbase = np.cand_entries;
+            np.cand_entries += nseg * static_cast<int64_t>(kk);
+            // Seed the global threshold from a sample when the segments' own
+            // k-th values would leave a large merge (many segments, large k).
+            const int64_t njobs = std::min<int64_t>(128, std::max<int64_t>(8, td.len >> 21));
+            const int64_t nchunks = 8;
+            const int64_t S = njobs * nchunks * kSampleChunk;
+            const int64_t stride = (td.len / (njobs * nchunks)) & ~int64_t(3);
+            const double lam = static_cast<double>(kk) * static_cast<double>(S) / static_cast<double>(td.len);
+            const int64_t r = static_cast<int64_t>(std::ceil(2.0 * lam + 4.0 * std::sqrt(lam) + 12.0));
+            if (allow_sample && nseg * static_cast<int64_t>(kk) >= 8192 && stride >= kSampleChunk && r <= 64) {
+                td.flags |= kTaskSampled;
+                for (int64_t j = 0; j < njobs; ++j) {
+                    SampleJob sj;
+                    sj.task = static_cast<int32_t>(t);
+                    sj.job_in_task = static_cast<int32_t>(j);
+                    sj.njobs = static_cast<int32_t>(njobs);
+                    sj.r = static_cast<int32_t>(r);
+                    sj.nchunks = static_cast<int32_t>(nchunks);
+                    sj.pad_ = 0;
+                    sj.pos0 = j * nchunks * stride;
+                    sj.stride = stride;
+                    sj.out_base = np.sample_entries;
+                    np.jobs.push_back(sj);
+                }
+                np.sample_entries += njobs * r;
+            }
+        }
         for (int64_t s = 0; s < nseg; ++s) {
             FusedSeg sg;
-            sg.start = off + s * seg_len;
+            sg.pos = static_cast<int32_t>(s * seg_len);
             int64_t e = std::min(td.len, (s + 1) * seg_len);
             sg.len = static_cast<int32_t>(e - s * seg_len);
             sg.task = static_cast<int32_t>(t);
             sg.seg_in_task = static_cast<int32_t>(s);
-            sg.pad_ = 0;
             np.segs.push_back(sg);
         }
         off += td.len;
@@ -241,13 +315,16 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     np.valid = true;
 
     // Device buffers.
-    const size_t state_bytes = kStateHeader + round_up(sizeof(uint64_t) * T, 16) + sizeof(uint32_t) * T;
-    const size_t desc_bytes = round_up(sizeof(FusedTask) * T, 256) + sizeof(FusedSeg) * np.segs.size();
-    cudaError_t e = ws->state.ensure(state_bytes);
+    const StateLayout L(T);
+    np.tasks_off = 0;
+    np.segs_off = round_up(sizeof(FusedTask) * T, 256);
+    np.jobs_off = np.segs_off + round_up(sizeof(FusedSeg) * np.segs.size(), 256);
+    const size_t desc_bytes = np.jobs_off + sizeof(SampleJob) * np.jobs.size();
+    cudaError_t e = ws->state.ensure(L.bytes);
     if (e == cudaSuccess) e = ws->desc.ensure(desc_bytes);
     if (e == cudaSuccess && np.fused) {
-        e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.slots) * kk);
-        if (e == cudaSuccess) e = ws->slot_cnt.ensure(sizeof(uint32_t) * static_cast<size_t>(np.slots));
+        e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.cand_entries));
+        if (e == cudaSuccess) e = ws->samples.ensure(sizeof(uint64_t) * static_cast<size_t>(np.sample_entries));
         if (e == cudaSuccess && kk > kBitonicMax)
             e = ws->scratch.ensure(sizeof(uint64_t) * static_cast<size_t>(np.grid) * kk);
     }
@@ -265,11 +342,20 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
         return fail(e == cudaErrorMemoryAllocation ? RADIK_ERR_OOM : RADIK_ERR_CUDA,
                     std::string("workspace allocation: ") + cudaGetErrorString(e));
     }
-    e = cudaMemcpy(ws->desc.p, np.tasks.data(), sizeof(FusedTask) * T, cudaMemcpyHostToDevice);
+    e = cudaMemcpy(ws->desc.as<char>(np.tasks_off), np.tasks.data(), sizeof(FusedTask) * T, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !np.segs.empty())
-        e = cudaMemcpy(ws->desc.as<char>(round_up(sizeof(FusedTask) * T, 256)), np.segs.data(),
-                       sizeof(FusedSeg) * np.segs.size(), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, state_bytes);
+        e = cudaMemcpy(ws->desc.as<char>(np.segs_off), np.segs.data(), sizeof(FusedSeg) * np.segs.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !np.jobs.empty())
+        e = cudaMemcpy(ws->desc.as<char>(np.jobs_off), np.jobs.data(), sizeof(SampleJob) * np.jobs.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, L.bytes);
+    if (e == cudaSuccess && np.fused && !np.jobs.empty()) {
+        SampleKernel sk = pick_sample(scale);
+        const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
+        e = cudaFuncSetAttribute(reinterpret_cast<const void*>(sk), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(ssmem));
+    }
     if (e != cudaSuccess) {
         pl.valid = false;
         return fail(RADIK_ERR_CUDA, std::string("plan upload: ") + cudaGetErrorString(e));
@@ -278,54 +364,70 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     return RADIK_OK;
 }
 
-const FusedTask* plan_tasks(radik_ws* ws) { return ws->desc.as<FusedTask>(0); }
-const FusedSeg* plan_segs(radik_ws* ws) {
-    return ws->desc.as<FusedSeg>(round_up(sizeof(FusedTask) * ws->plan.T, 256));
-}
-
 FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, const float* vin, const void* iin,
                          int64_t k, uint32_t flags) {
     const Plan& pl = ws->plan;
+    const StateLayout L(pl.T);
     FusedParams p;
     std::memset(&p, 0, sizeof(p));
     p.data = vin;
-    p.tasks = plan_tasks(ws);
-    p.segs = plan_segs(ws);
+    p.tasks = ws->desc.as<FusedTask>(pl.tasks_off);
+    p.segs = ws->desc.as<FusedSeg>(pl.segs_off);
+    p.task_io = nullptr;
     p.nsegs = pl.nsegs;
-    p.k = static_cast<uint32_t>(k);
+    p.kmax = static_cast<uint32_t>(k);
     p.cap = pl.cap;
-    p.ascend = (flags & RADIK_ASCEND) ? 1 : 0;
-    p.sp = make_score_params((flags & RADIK_LARGEST) != 0, (flags & RADIK_WITHSCALE) != 0);
+    p.retry = 0;
     p.idx_in = (flags & RADIK_WITHIDXIN) ? iin : nullptr;
     p.idx_bytes = idx_bytes;
     p.val_out = vout;
     p.idx_out = iout;
     p.err = err_ptr(ws);
-    p.work_counter = ws->state.as<uint32_t>(4);
-    p.gthr = ws->state.as<uint64_t>(kStateHeader);
-    p.task_done = ws->state.as<uint32_t>(kStateHeader + round_up(sizeof(uint64_t) * pl.T, 16));
+    p.work_counter = ws->state.as<uint32_t>(StateLayout::kWork);
+    p.gthr = ws->state.as<uint64_t>(L.gthr);
+    p.task_done = ws->state.as<uint32_t>(L.done);
+    p.task_cnt = ws->state.as<uint32_t>(L.cnt);
+    p.fail = ws->state.as<uint32_t>(L.fail);
     p.cand = ws->cand.as<uint64_t>();
-    p.slot_cnt = ws->slot_cnt.as<uint32_t>();
     p.sort_scratch = ws->scratch.as<uint64_t>();
     return p;
 }
 
 int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s) {
     const Plan& pl = ws->plan;
-    // Reset per-call counters: err stays (sticky until read), work counter,
-    // thresholds and done counters are zeroed.
-    RADIK_CUDA(cudaMemsetAsync(ws->state.as<char>(4), 0,
-                               kStateHeader - 4 + round_up(sizeof(uint64_t) * pl.T, 16) + sizeof(uint32_t) * pl.T, s));
-    FusedKernel fk = pick_fused(pl.threads, pl.vec, (flags & RADIK_WITHSCALE) != 0);
+    const StateLayout L(pl.T);
+    const bool scale = (flags & RADIK_WITHSCALE) != 0;
+    // Reset the per-call state (the error word stays sticky until read).
+    RADIK_CUDA(cudaMemsetAsync(ws->state.as<char>(StateLayout::kWork), 0, L.bytes - StateLayout::kWork, s));
+    if (!pl.jobs.empty()) {
+        SampleKernel sk = pick_sample(scale);
+        const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
+        sk<<<static_cast<unsigned>(pl.jobs.size()), 256, ssmem, s>>>(
+            p, ws->desc.as<SampleJob>(pl.jobs_off), ws->samples.as<uint64_t>(), ws->state.as<uint32_t>(L.sdone));
+        RADIK_CUDA(cudaGetLastError());
+    }
+    FusedKernel fk = pick_fused(pl.threads, pl.vec, scale);
     fk<<<pl.grid, pl.threads, pl.smem, s>>>(p);
     RADIK_CUDA(cudaGetLastError());
+    if (!pl.jobs.empty()) {
+        // Recompute, without the sampled threshold, any task whose seeded
+        // threshold left fewer than k candidates; exits at once otherwise.
+        FusedParams r = p;
+        r.retry = 1;
+        r.work_counter = ws->state.as<uint32_t>(StateLayout::kWorkRetry);
+        r.gthr = ws->state.as<uint64_t>(L.gthr_r);
+        r.task_done = ws->state.as<uint32_t>(L.done_r);
+        r.task_cnt = ws->state.as<uint32_t>(L.cnt_r);
+        fk<<<pl.grid, pl.threads, pl.smem, s>>>(r);
+        RADIK_CUDA(cudaGetLastError());
+    }
     return RADIK_OK;
 }
 
 int run_plain(radik_ws* ws, const FusedParams& fp, uint32_t flags, cudaStream_t s) {
     const Plan& pl = ws->plan;
     const int64_t T = pl.T;
-    const uint32_t k = fp.k;
+    const uint32_t k = fp.kmax;
     const bool scale = (flags & RADIK_WITHSCALE) != 0;
     PlainParams p;
     std::memset(&p, 0, sizeof(p));
@@ -335,14 +437,14 @@ int run_plain(radik_ws* ws, const FusedParams& fp, uint32_t flags, cudaStream_t 
     p.nsegs = pl.nsegs;
     p.ntasks = static_cast<int32_t>(T);
     p.k = k;
-    p.sp = fp.sp;
+    p.sp = make_score_params((flags & RADIK_LARGEST) != 0, scale);
     p.hist = ws->hist.as<uint32_t>();
     p.st = ws->pstate.as<PlainState>();
     p.out_stage = ws->stage.as<uint64_t>();
     p.cand[0] = ws->pcand[0].as<uint64_t>();
     p.cand[1] = ws->pcand[1].as<uint64_t>();
     p.err = fp.err;
-    uint32_t* any = ws->state.as<uint32_t>(8);
+    uint32_t* any = ws->state.as<uint32_t>(StateLayout::kAny);
     const DeviceInfo di = device_info();
     const int grid_in = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(pl.nsegs, 8LL * di.sms)));
 
@@ -463,8 +565,7 @@ int radik_ws_create(int64_t n, int64_t num_tasks, int index_bytes, radik_ws** ou
         return fail(RADIK_ERR_OOM, "pinned allocation failed");
     }
     *ws->h_err = 0;
-    const size_t sb = kStateHeader + round_up(sizeof(uint64_t) * std::max<int64_t>(num_tasks, 1), 16) +
-                      sizeof(uint32_t) * std::max<int64_t>(num_tasks, 1);
+    const size_t sb = StateLayout(num_tasks).bytes;
     if (ws->state.ensure(sb) != cudaSuccess || cudaMemset(ws->state.p, 0, sb) != cudaSuccess) {
         cudaFreeHost(ws->h_err);
         delete ws;
@@ -476,7 +577,7 @@ int radik_ws_create(int64_t n, int64_t num_tasks, int index_bytes, radik_ws** ou
 
 int radik_ws_destroy(radik_ws* ws) {
     if (!ws) return RADIK_OK;
-    for (DevBuf* b : {&ws->state, &ws->desc, &ws->cand, &ws->slot_cnt, &ws->scratch, &ws->hist, &ws->pstate,
+    for (DevBuf* b : {&ws->state, &ws->desc, &ws->cand, &ws->samples, &ws->scratch, &ws->hist, &ws->pstate,
                       &ws->stage, &ws->pcand[0], &ws->pcand[1], &ws->io_in, &ws->io_idx, &ws->io_vout, &ws->io_iout})
         b->release();
     if (ws->h_err) cudaFreeHost(ws->h_err);
@@ -487,7 +588,7 @@ int radik_ws_destroy(radik_ws* ws) {
 int radik_ws_bytes(const radik_ws* ws, size_t* bytes) {
     if (!ws || !bytes) return fail(RADIK_ERR_INVALID, "NULL argument");
     size_t b = 0;
-    for (const DevBuf* d : {&ws->state, &ws->desc, &ws->cand, &ws->slot_cnt, &ws->scratch, &ws->hist, &ws->pstate,
+    for (const DevBuf* d : {&ws->state, &ws->desc, &ws->cand, &ws->samples, &ws->scratch, &ws->hist, &ws->pstate,
                             &ws->stage, &ws->pcand[0], &ws->pcand[1], &ws->io_in, &ws->io_idx, &ws->io_vout,
                             &ws->io_iout})
         b += d->bytes;

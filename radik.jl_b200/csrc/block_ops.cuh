@@ -19,7 +19,7 @@ namespace radik {
 template <int THREADS>
 struct BlockScratch {
     static constexpr int kWarps = THREADS / 32;
-    uint32_t hist[256];
+    uint32_t hist[2048];
     uint32_t warp_u32[kWarps];
     uint64_t warp_a[kWarps];
     uint64_t warp_b[kWarps];
@@ -95,91 +95,50 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
     return before + inc - v;
 }
 
-// Rank search over a 256-bin histogram from the top bin (select_bin.jl:
-// warp scan + find_bin_and_write!, here one warp with 8 bins per lane):
-// returns bin b with above(b) < r <= above(b) + hist[b]; writes residual rank
-// and the bin count.  Executed by warp 0; result broadcast through s.bc32.
+// Rank search over a histogram of nb (<= 2048) bins counted from the top bin
+// (the role of select_bin_kernel!'s scan + find_bin_and_write!,
+// select_bin.jl:125-159, 268-348).  Thread i owns bins nb-1-i*per down to
+// nb-(i+1)*per; a block scan gives the count above each thread's range and the
+// owner of rank r writes (bin, residual rank, bin count, count above the bin)
+// to s.bc32 (bin count 0xffffffff when r exceeds the total).  All threads call.
 template <int THREADS>
-__device__ __forceinline__ void block_rank_search(uint32_t r, uint32_t nbins, BlockScratch<THREADS>& s) {
-    if (threadIdx.x < 32) {
-        const uint32_t lane = lane_id();
-        if (lane == 0) { s.bc32[0] = 0; s.bc32[1] = 0; s.bc32[2] = 0xffffffffu; }
-        __syncwarp();
-        const uint32_t per = (nbins + 31) / 32;
-        uint32_t c[8];
-        uint32_t sum = 0;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            uint32_t b = lane * per + j;
-            c[j] = (j < static_cast<int>(per) && b < nbins) ? s.hist[b] : 0u;
-            sum += c[j];
-        }
-        uint32_t incl = warp_inclusive_scan<false>(sum);  // suffix sum from this lane up
-        uint32_t above = incl - sum;
-        if (above < r && r <= incl) {
-            uint32_t rr = r - above;
-#pragma unroll
-            for (int j = 7; j >= 0; --j) {
-                if (j < static_cast<int>(per) && c[j] > 0) {
-                    if (c[j] >= rr) {
-                        s.bc32[0] = lane * per + j;
-                        s.bc32[1] = rr;
-                        s.bc32[2] = c[j];
-                        rr = 0;
-                        break;
-                    }
-                    rr -= c[j];
-                }
+__device__ __forceinline__ void block_rank_search(uint32_t r, uint32_t nb, BlockScratch<THREADS>& s) {
+    const uint32_t per = (nb + THREADS - 1) / THREADS;
+    if (threadIdx.x == 0) { s.bc32[0] = 0; s.bc32[1] = 0; s.bc32[2] = 0xffffffffu; s.bc32[3] = 0; }
+    uint32_t sum = 0;
+    for (uint32_t j = 0; j < per; ++j) {
+        uint32_t rb = threadIdx.x * per + j;
+        if (rb < nb) sum += s.hist[nb - 1 - rb];
+    }
+    uint32_t total;
+    const uint32_t before = block_exclusive_scan<THREADS>(sum, &total, s);
+    if (before < r && r <= before + sum) {
+        uint32_t rr = r - before;
+        for (uint32_t j = 0; j < per; ++j) {
+            uint32_t rb = threadIdx.x * per + j;
+            if (rb >= nb) break;
+            uint32_t c = s.hist[nb - 1 - rb];
+            if (c > 0 && c >= rr) {
+                s.bc32[0] = nb - 1 - rb;
+                s.bc32[1] = rr;
+                s.bc32[2] = c;
+                s.bc32[3] = r - rr;
+                break;
             }
+            rr -= c;
         }
     }
     __syncthreads();
 }
 
-// Exact top-k of buf[0, cnt) (unique composites; cnt > k >= 1).  On return
-// buf[0, k) holds the k largest composites in their previous relative order
-// and the smallest of them is returned.  All threads must call.
+// Ordered in-place compaction: moves the entries of buf[0, cnt) that are
+// >= keep_from to the front (previous order kept).  Returns their number;
+// *mn receives their minimum (~0 when none).
 template <int THREADS>
-__device__ __forceinline__ uint64_t block_select_topk(uint64_t* buf, uint32_t cnt, uint32_t k, BlockScratch<THREADS>& s,
-                                      uint32_t* err) {
-    const int tid = threadIdx.x;
-    // Highest bit where the composites differ.
-    uint64_t vor = 0, vand = ~0ull;
-    for (uint32_t i = tid; i < cnt; i += THREADS) { uint64_t c = buf[i]; vor |= c; vand &= c; }
-    block_or_and<THREADS>(vor, vand, s);
-    const uint64_t diff = vor ^ vand;
-    int top = 63 - __clzll(static_cast<long long>(diff));  // diff != 0 since cnt >= 2
-    uint64_t prefix = (top >= 63) ? 0ull : (vand >> (top + 1));
-    int pbits = 63 - top;  // number of prefix bits (above `top`)
-    uint32_t r = k;
-    uint64_t keep_from = 0;
-    for (int guard = 0; guard < 64; ++guard) {
-        const int w = top + 1 < 8 ? top + 1 : 8;
-        const int sh = top + 1 - w;
-        for (int i = tid; i < 256; i += THREADS) s.hist[i] = 0;
-        __syncthreads();
-        const uint64_t dmask = (1ull << w) - 1;
-        for (uint32_t i = tid; i < cnt; i += THREADS) {
-            uint64_t c = buf[i];
-            bool match = (pbits == 0) || ((c >> (sh + w)) == prefix);
-            if (match) atomicAdd(&s.hist[(c >> sh) & dmask], 1u);
-        }
-        __syncthreads();
-        block_rank_search<THREADS>(r, 1u << w, s);
-        const uint32_t b = s.bc32[0], rr = s.bc32[1], cb = s.bc32[2];
-        __syncthreads();
-        prefix = (pbits == 0) ? b : ((prefix << w) | b);
-        pbits += w;
-        r = rr;
-        if (cb == rr || sh == 0) {
-            if (cb != rr && tid == 0) record_error(err, kErrInternal);
-            keep_from = prefix << sh;
-            break;
-        }
-        top = sh - 1;
-    }
-    // Ordered in-place compaction of the kept composites to the front.
+__device__ __forceinline__ uint32_t block_compact_ge(uint64_t* buf, uint32_t cnt, uint64_t keep_from,
+                                                     BlockScratch<THREADS>& s, uint64_t* mn_out) {
     constexpr int E = 4;
+    const int tid = threadIdx.x;
     uint64_t mn = ~0ull;
     uint32_t out = 0;
     for (uint32_t base = 0; base < cnt; base += THREADS * E) {
@@ -207,19 +166,97 @@ __device__ __forceinline__ uint64_t block_select_topk(uint64_t* buf, uint32_t cn
         out += total;
         __syncthreads();
     }
-    if (out != k && tid == 0) record_error(err, kErrInternal);
-    return block_min_u64<THREADS>(mn, s);
+    *mn_out = block_min_u64<THREADS>(mn, s);
+    return out;
 }
 
-// Ascending bitonic sort of a[0, n) in shared memory, n a power of two.
+// Narrows buf[0, cnt) (unique composites, all inside [lo, hi]) to the entries
+// >= keep_from, the lower edge of the digit bin that holds rank k counted from
+// the largest: the countBin -> selectBin -> selectCandidate cycle of
+// count_bin.jl, select_bin.jl and select_candidate.jl run on on-chip data.
+// Digits are 11-bit windows starting right below the common prefix of lo and
+// hi; windows are refined until at most max_keep (>= k) entries would remain,
+// so max_keep == k yields exactly the top k.  Kept entries move to the front.
+// Returns their number (cnt when cnt <= k); *keep_from_out and *mn_out receive
+// the threshold and the smallest kept composite.  All threads must call.
 template <int THREADS>
-__device__ __forceinline__ void bitonic_sort_u64(uint64_t* a, uint32_t n) {
+__device__ uint32_t block_shrink(uint64_t* buf, uint32_t cnt, uint32_t k, uint32_t max_keep, uint64_t lo,
+                                 uint64_t hi, BlockScratch<THREADS>& s, uint32_t* err, uint64_t* keep_from_out,
+                                 uint64_t* mn_out) {
+    constexpr int W = 11;
+    const int tid = threadIdx.x;
+    const uint64_t diff = lo ^ hi;
+    if (cnt <= k || diff == 0) {
+        *keep_from_out = lo;
+        uint64_t mn = ~0ull;
+        for (uint32_t i = tid; i < cnt; i += THREADS) mn = buf[i] < mn ? buf[i] : mn;
+        *mn_out = block_min_u64<THREADS>(mn, s);
+        return cnt;
+    }
+    int top = 63 - __clzll(static_cast<long long>(diff));
+    uint64_t prefix = (top >= 63) ? 0ull : (hi >> (top + 1));
+    int pbits = 63 - top;  // bits above `top` shared by every entry
+    uint32_t r = k, above_total = 0;
+    uint64_t keep_from = lo;
+    for (int guard = 0; guard < 8; ++guard) {
+        const int w = top + 1 < W ? top + 1 : W;
+        const int sh = top + 1 - w;
+        const uint32_t nb = 1u << w;
+        for (uint32_t i = tid; i < nb; i += THREADS) s.hist[i] = 0;
+        __syncthreads();
+        const uint64_t dmask = nb - 1;
+        for (uint32_t i = tid; i < cnt; i += THREADS) {
+            uint64_t c = buf[i];
+            if (pbits == 0 || (c >> (sh + w)) == prefix) atomicAdd(&s.hist[(c >> sh) & dmask], 1u);
+        }
+        __syncthreads();
+        block_rank_search<THREADS>(r, nb, s);
+        const uint32_t b = s.bc32[0], rr = s.bc32[1], cb = s.bc32[2], ab = s.bc32[3];
+        __syncthreads();
+        if (cb == 0xffffffffu) {  // rank beyond the entries: inputs outside [lo, hi]
+            if (tid == 0) record_error(err, kErrInternal);
+            keep_from = lo;
+            break;
+        }
+        prefix = (pbits == 0) ? b : ((prefix << w) | b);
+        pbits += w;
+        above_total += ab;
+        r = rr;
+        if (above_total + cb <= max_keep || sh == 0) {
+            keep_from = prefix << sh;
+            break;
+        }
+        top = sh - 1;
+    }
+    *keep_from_out = keep_from;
+    return block_compact_ge<THREADS>(buf, cnt, keep_from, s, mn_out);
+}
+
+// Exact top-k of buf[0, cnt) (unique composites): on return buf[0, min(cnt,k))
+// holds the k largest in their previous order; returns their number and the
+// smallest of them (the k-th composite) through *kth.
+template <int THREADS>
+__device__ uint32_t block_select_topk(uint64_t* buf, uint32_t cnt, uint32_t k, BlockScratch<THREADS>& s,
+                                      uint32_t* err, uint64_t* kth) {
+    uint64_t vor = 0, vand = ~0ull;
+    for (uint32_t i = threadIdx.x; i < cnt; i += THREADS) { uint64_t c = buf[i]; vor |= c; vand &= c; }
+    block_or_and<THREADS>(vor, vand, s);
+    uint64_t kf;
+    uint32_t kept = block_shrink<THREADS>(buf, cnt, k, k, vand, vor, s, err, &kf, kth);
+    if (cnt > k && kept != k && threadIdx.x == 0) record_error(err, kErrInternal);
+    return kept;
+}
+
+// Bitonic sort of a[0, n) in shared memory (n a power of two), ascending or
+// descending.
+template <int THREADS>
+__device__ __forceinline__ void bitonic_sort_u64(uint64_t* a, uint32_t n, bool descending = false) {
     for (uint32_t size = 2; size <= n; size <<= 1) {
         for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
             for (uint32_t i = threadIdx.x; i < (n >> 1); i += THREADS) {
                 uint32_t lo = 2 * i - (i & (stride - 1));
                 uint32_t hi = lo + stride;
-                bool asc = (lo & size) == 0;
+                bool asc = ((lo & size) == 0) != descending;
                 uint64_t x = a[lo], y = a[hi];
                 if ((x > y) == asc) { a[lo] = y; a[hi] = x; }
             }

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(THREADS) plain_hist_input(PlainParams p) {
         __syncthreads();
         const float scaler = kScale ? task_scaler(p.data, td.start, td.len, 1) : 0.0f;
         for (int64_t i = threadIdx.x; i < sg.len; i += THREADS) {
-            uint32_t bits = __float_as_uint(p.data[sg.start + i]);
+            uint32_t bits = __float_as_uint(p.data[td.start + sg.pos + i]);
             uint32_t s = score_of<kScale>(bits, scaler, p.sp);
             atomicAdd(&h[s >> 20], 1u);
         }
@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(THREADS) plain_compact_input(PlainParams p) {
         const bool allwin = copy_all ? true : (p.st[t].allwin != 0);
         uint32_t* nnext = &p.st[t].nnext;
         for (int64_t i = threadIdx.x; i < sg.len; i += THREADS) {
-            const int64_t g = sg.start + i;
+            const int64_t g = td.start + sg.pos + i;
             uint32_t bits = __float_as_uint(p.data[g]);
             uint32_t s = score_of<kScale>(bits, scaler, p.sp);
             uint64_t c = make_composite(s, static_cast<uint32_t>(g - td.start));
@@ -233,49 +233,31 @@ __global__ void __launch_bounds__(THREADS) plain_finalize(PlainParams p, FusedPa
     __shared__ FusedShared<THREADS> sh;
     const int t = blockIdx.x;
     const FusedTask td = p.tasks[t];
+    const TaskView tv = task_view<false>(fp, t, td);
     const uint32_t m = td.len < static_cast<int64_t>(p.k) ? static_cast<uint32_t>(td.len) : p.k;
     if (threadIdx.x == 0 && p.st[t].nout != m) record_error(p.err, kErrInternal);
     const uint64_t* row = p.out_stage + static_cast<int64_t>(t) * p.k;
     if (m <= kBitonicMax) {
         for (uint32_t i = threadIdx.x; i < m; i += THREADS) s_buf[i] = row[i];
         __syncthreads();
-        finish_task<THREADS>(fp, t, td, s_buf, m, sh);
+        finish_task<THREADS>(fp, tv, s_buf, m, sh);
     } else {
         // Sort keys built in the task's staging row, radix-sorted with a
-        // scratch row; then the shared output code path.
+        // scratch row, then the shared row writer.
         uint64_t* a = p.out_stage + static_cast<int64_t>(t) * p.k;
         uint64_t* b = scratch + static_cast<int64_t>(t) * p.k;
         for (uint32_t i = threadIdx.x; i < m; i += THREADS) {
             uint32_t pos = composite_pos(a[i]);
             if (pos >= static_cast<uint64_t>(td.len)) { record_error(p.err, kErrBounds); pos = 0; }
-            uint32_t bits = __float_as_uint(p.data[td.start + pos]);
-            a[i] = output_sort_key(bits, pos, p.sp, fp.ascend != 0);
+            uint32_t bits = __float_as_uint(tv.data[pos]);
+            a[i] = output_sort_key(bits, pos, tv.sp, tv.ascend);
         }
         __syncthreads();
         uint32_t* wd = reinterpret_cast<uint32_t*>(s_buf);
         uint32_t* db = wd + (THREADS / 32) * 256;
         uint64_t* sorted = radix_sort_u64<THREADS>(a, b, m, sh.bs, wd, db);
         __syncthreads();
-        float* vrow = fp.val_out + static_cast<int64_t>(t) * p.k;
-        for (uint32_t j = threadIdx.x; j < p.k; j += THREADS) {
-            float v = 0.0f;
-            int64_t idx = -1;
-            if (j < m) {
-                uint32_t pos = static_cast<uint32_t>(sorted[j]);
-                if (pos >= static_cast<uint64_t>(td.len)) pos = 0;
-                int64_t g = td.start + pos;
-                v = p.data[g];
-                if (fp.idx_in) {
-                    idx = (fp.idx_bytes == 8) ? static_cast<const int64_t*>(fp.idx_in)[g]
-                                              : static_cast<int64_t>(static_cast<const int32_t*>(fp.idx_in)[g]);
-                } else {
-                    idx = static_cast<int64_t>(pos) + 1;
-                }
-            }
-            vrow[j] = v;
-            if (fp.idx_bytes == 8) static_cast<int64_t*>(fp.idx_out)[static_cast<int64_t>(t) * p.k + j] = idx;
-            else static_cast<int32_t*>(fp.idx_out)[static_cast<int64_t>(t) * p.k + j] = static_cast<int32_t>(idx);
-        }
+        write_row<THREADS>(fp, tv, sorted, m);
     }
 }
 

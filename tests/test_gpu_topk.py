@@ -186,3 +186,33 @@ def test_deterministic_alone_and_in_batch(radik, torch_cuda):
         assert np.array_equal(av[0].view(np.uint32), bv[t].view(np.uint32))
         assert np.array_equal(ai[0], bi[t])
         off += n
+
+
+def test_sampled_threshold_retry(oracle, radik, torch_cuda, monkeypatch):
+    """Large values planted exactly where the multi-segment sampler reads
+    (64 chunks of 512 at multiples of 16384 for n = 2^20 with 16384-element
+    segments) make the seeded threshold too high; the retry launch must still
+    return the exact answer."""
+    monkeypatch.setenv("RADIK_SEG", "16384")
+    n = 1 << 20
+    rng = np.random.default_rng(31)
+    x = rng.random(n, dtype=np.float32)
+    for m in range(64):
+        x[m * 16384:m * 16384 + 512] = 100.0 + rng.random(512, dtype=np.float32)
+    for k in (256, 1000):
+        _compare(oracle, radik, torch_cuda, x, [n], k)
+        _compare(oracle, radik, torch_cuda, x, [n], k, largest=False)
+
+
+def test_in_block_sample_redo(oracle, radik, torch_cuda):
+    """Large values planted where the in-block sampler of a single-segment
+    task reads (16 chunks of 64 at multiples of len/16) force the redo path."""
+    n = 1 << 16
+    rng = np.random.default_rng(37)
+    x = rng.random(n, dtype=np.float32)
+    for c in range(16):
+        x[c * (n // 16):c * (n // 16) + 64] = 50.0 + rng.random(64, dtype=np.float32)
+    lens = [n, n]
+    data = np.concatenate([x, x[::-1].copy()])
+    for k in (64, 256, 1024):
+        _compare(oracle, radik, torch_cuda, data, lens, k)
