@@ -78,7 +78,7 @@ size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 // Fused kernel dispatch
 // ---------------------------------------------------------------------------
 using FusedKernel = void (*)(FusedParams);
-constexpr int kStages = 4;  // TMA ring depth of the fused kernel
+constexpr int kStages = 6;  // TMA ring depth of the fused kernel
 
 template <int T, int V, bool S>
 FusedKernel fused_ptr() { return fused_topk_kernel<T, V, kStages, S>; }
@@ -182,12 +182,14 @@ struct StateLayout {
 
 uint32_t* err_ptr(radik_ws* ws) { return ws->state.as<uint32_t>(StateLayout::kErr); }
 
-// Shared-buffer capacity of the fused kernel: k entries, one tile of
-// appends, and headroom so that a mid-stream shrink frees room for many
-// tiles of candidates.
+// Shared-buffer capacity of the fused kernel: a settled region that holds
+// k entries plus the slack of a mid-stream shrink, followed by the per-warp
+// candidate regions (kRegionEntries).  Candidates that find no room are
+// re-offered after a shrink, so no region needs to hold a whole tile.
 size_t fused_cap(size_t k, size_t tile, int threads) {
-    size_t headroom = std::max<size_t>({k / 2, tile, 1024});
-    size_t cap = k + tile + 8 + headroom;
+    (void)tile;
+    size_t cap_s = round_up(k + std::max<size_t>(k / 4, 512), 64);
+    size_t cap = cap_s + kRegionEntries;
     size_t p2 = 1;
     while (p2 < std::min<size_t>(k, kBitonicMax)) p2 <<= 1;
     cap = std::max(cap, p2);

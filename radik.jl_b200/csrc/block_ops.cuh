@@ -19,7 +19,7 @@ namespace radik {
 template <int THREADS>
 struct BlockScratch {
     static constexpr int kWarps = THREADS / 32;
-    uint32_t hist[2048];
+    uint32_t hist[256];
     uint32_t warp_u32[kWarps];
     uint64_t warp_a[kWarps];
     uint64_t warp_b[kWarps];
@@ -29,6 +29,15 @@ struct BlockScratch {
 
 __device__ __forceinline__ uint64_t shfl_xor_u64(uint64_t v, int m) {
     return __shfl_xor_sync(kFullMask, static_cast<unsigned long long>(v), m);
+}
+
+// Histogram increment with the lanes of a warp that hit the same bin
+// combined into one shared atomic (same-bin lanes would otherwise serialise).
+// All lanes of the warp must call; lanes with valid == false add nothing.
+__device__ __forceinline__ void warp_hist_add(uint32_t* hist, uint32_t bin, bool valid) {
+    const uint32_t key = valid ? bin : 0xffffffffu;
+    const uint32_t peers = __match_any_sync(kFullMask, key);
+    if (valid && (lanemask_lt() & peers) == 0) atomicAdd(hist + bin, static_cast<uint32_t>(__popc(peers)));
 }
 
 // OR and AND of v over the block; result visible to all threads.
@@ -95,37 +104,45 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
     return before + inc - v;
 }
 
-// Rank search over a histogram of nb (<= 2048) bins counted from the top bin
-// (the role of select_bin_kernel!'s scan + find_bin_and_write!,
-// select_bin.jl:125-159, 268-348).  Thread i owns bins nb-1-i*per down to
-// nb-(i+1)*per; a block scan gives the count above each thread's range and the
-// owner of rank r writes (bin, residual rank, bin count, count above the bin)
-// to s.bc32 (bin count 0xffffffff when r exceeds the total).  All threads call.
+// Rank search over a histogram of nb (<= 256) bins counted from the top bin
+// (the role of select_bin_kernel!'s warp scan + find_bin_and_write!,
+// select_bin.jl:125-159, 268-348).  Warp 0 does it: lane l owns bins
+// nb-1-l*per .. nb-(l+1)*per, a suffix warp scan gives the count above each
+// lane's range, and the owner of rank r writes (bin, residual rank, bin count,
+// count above the bin) to s.bc32 (bin count 0xffffffff when r exceeds the
+// total).  All threads must call (the result is published by a barrier).
 template <int THREADS>
 __device__ __forceinline__ void block_rank_search(uint32_t r, uint32_t nb, BlockScratch<THREADS>& s) {
-    const uint32_t per = (nb + THREADS - 1) / THREADS;
-    if (threadIdx.x == 0) { s.bc32[0] = 0; s.bc32[1] = 0; s.bc32[2] = 0xffffffffu; s.bc32[3] = 0; }
-    uint32_t sum = 0;
-    for (uint32_t j = 0; j < per; ++j) {
-        uint32_t rb = threadIdx.x * per + j;
-        if (rb < nb) sum += s.hist[nb - 1 - rb];
-    }
-    uint32_t total;
-    const uint32_t before = block_exclusive_scan<THREADS>(sum, &total, s);
-    if (before < r && r <= before + sum) {
-        uint32_t rr = r - before;
-        for (uint32_t j = 0; j < per; ++j) {
-            uint32_t rb = threadIdx.x * per + j;
-            if (rb >= nb) break;
-            uint32_t c = s.hist[nb - 1 - rb];
-            if (c > 0 && c >= rr) {
-                s.bc32[0] = nb - 1 - rb;
-                s.bc32[1] = rr;
-                s.bc32[2] = c;
-                s.bc32[3] = r - rr;
-                break;
+    if (threadIdx.x < 32) {
+        const uint32_t lane = lane_id();
+        const uint32_t per = (nb + 31) / 32;  // <= 8
+        uint32_t c[8];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t rb = lane * per + j;
+            c[j] = (j < static_cast<int>(per) && rb < nb) ? s.hist[nb - 1 - rb] : 0u;
+            sum += c[j];
+        }
+        const uint32_t incl = warp_inclusive_scan<true>(sum);  // count in lanes <= this one
+        const uint32_t before = incl - sum;
+        const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+        if (lane == 0 && r > total) { s.bc32[0] = 0; s.bc32[1] = 0; s.bc32[2] = 0xffffffffu; s.bc32[3] = 0; }
+        if (before < r && r <= incl) {
+            uint32_t rr = r - before;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (j < static_cast<int>(per) && c[j] > 0) {
+                    if (c[j] >= rr) {
+                        s.bc32[0] = nb - 1 - (lane * per + j);
+                        s.bc32[1] = rr;
+                        s.bc32[2] = c[j];
+                        s.bc32[3] = r - rr;
+                        break;
+                    }
+                    rr -= c[j];
+                }
             }
-            rr -= c;
         }
     }
     __syncthreads();
@@ -174,16 +191,18 @@ __device__ __forceinline__ uint32_t block_compact_ge(uint64_t* buf, uint32_t cnt
 // >= keep_from, the lower edge of the digit bin that holds rank k counted from
 // the largest: the countBin -> selectBin -> selectCandidate cycle of
 // count_bin.jl, select_bin.jl and select_candidate.jl run on on-chip data.
-// Digits are 11-bit windows starting right below the common prefix of lo and
+// Digits are 8-bit windows starting right below the common prefix of lo and
 // hi; windows are refined until at most max_keep (>= k) entries would remain,
-// so max_keep == k yields exactly the top k.  Kept entries move to the front.
-// Returns their number (cnt when cnt <= k); *keep_from_out and *mn_out receive
-// the threshold and the smallest kept composite.  All threads must call.
+// so max_keep == k yields exactly the top k.  Between windows the buffer is
+// compacted to the entries that can still be kept, so refinements scan only
+// those.  Kept entries move to the front (previous order).  Returns their
+// number (cnt when cnt <= k); *keep_from_out and *mn_out receive the
+// threshold and the smallest kept composite.  All threads must call.
 template <int THREADS>
 __device__ uint32_t block_shrink(uint64_t* buf, uint32_t cnt, uint32_t k, uint32_t max_keep, uint64_t lo,
                                  uint64_t hi, BlockScratch<THREADS>& s, uint32_t* err, uint64_t* keep_from_out,
                                  uint64_t* mn_out) {
-    constexpr int W = 11;
+    constexpr int W = 8;
     const int tid = threadIdx.x;
     const uint64_t diff = lo ^ hi;
     if (cnt <= k || diff == 0) {
@@ -195,19 +214,21 @@ __device__ uint32_t block_shrink(uint64_t* buf, uint32_t cnt, uint32_t k, uint32
     }
     int top = 63 - __clzll(static_cast<long long>(diff));
     uint64_t prefix = (top >= 63) ? 0ull : (hi >> (top + 1));
-    int pbits = 63 - top;  // bits above `top` shared by every entry
-    uint32_t r = k, above_total = 0;
+    int pbits = 63 - top;  // bits above `top` shared by the entries still in play
+    uint32_t r = k, above_total = 0, n = cnt;
     uint64_t keep_from = lo;
-    for (int guard = 0; guard < 8; ++guard) {
+    for (int guard = 0; guard < 9; ++guard) {
         const int w = top + 1 < W ? top + 1 : W;
         const int sh = top + 1 - w;
         const uint32_t nb = 1u << w;
         for (uint32_t i = tid; i < nb; i += THREADS) s.hist[i] = 0;
         __syncthreads();
         const uint64_t dmask = nb - 1;
-        for (uint32_t i = tid; i < cnt; i += THREADS) {
-            uint64_t c = buf[i];
-            if (pbits == 0 || (c >> (sh + w)) == prefix) atomicAdd(&s.hist[(c >> sh) & dmask], 1u);
+        for (uint32_t base = 0; base < n; base += THREADS) {
+            const uint32_t i = base + tid;
+            const uint64_t c = i < n ? buf[i] : 0ull;
+            const bool in = i < n && (pbits == 0 || (c >> (sh + w)) == prefix);
+            warp_hist_add(s.hist, static_cast<uint32_t>((c >> sh) & dmask), in);
         }
         __syncthreads();
         block_rank_search<THREADS>(r, nb, s);
@@ -222,14 +243,61 @@ __device__ uint32_t block_shrink(uint64_t* buf, uint32_t cnt, uint32_t k, uint32
         pbits += w;
         above_total += ab;
         r = rr;
-        if (above_total + cb <= max_keep || sh == 0) {
-            keep_from = prefix << sh;
-            break;
+        keep_from = prefix << sh;
+        if (above_total + cb <= max_keep || sh == 0) break;
+        if (2 * (above_total + cb) < n) {  // drop what can no longer be kept
+            uint64_t mn;
+            n = block_compact_ge<THREADS>(buf, n, keep_from, s, &mn);
         }
         top = sh - 1;
     }
     *keep_from_out = keep_from;
-    return block_compact_ge<THREADS>(buf, cnt, keep_from, s, mn_out);
+    return block_compact_ge<THREADS>(buf, n, keep_from, s, mn_out);
+}
+
+// Lower edge of the digit bin holding rank r (from the largest) among
+// buf[0, n) (unique composites inside [lo, hi]): at least r entries are >= it,
+// and at most about `slack` when two windows suffice.  The buffer is left as
+// it is.  All threads must call.
+template <int THREADS>
+__device__ uint64_t block_rank_threshold(const uint64_t* buf, uint32_t n, uint32_t r, uint32_t slack, uint64_t lo,
+                                         uint64_t hi, BlockScratch<THREADS>& s) {
+    constexpr int W = 8;
+    const int tid = threadIdx.x;
+    const uint64_t diff = lo ^ hi;
+    if (n <= r || diff == 0) return lo;
+    int top = 63 - __clzll(static_cast<long long>(diff));
+    uint64_t prefix = (top >= 63) ? 0ull : (hi >> (top + 1));
+    int pbits = 63 - top;
+    uint32_t above_total = 0;
+    uint64_t keep_from = lo;
+    for (int pass = 0; pass < 2; ++pass) {
+        const int w = top + 1 < W ? top + 1 : W;
+        const int sh = top + 1 - w;
+        const uint32_t nb = 1u << w;
+        for (uint32_t i = tid; i < nb; i += THREADS) s.hist[i] = 0;
+        __syncthreads();
+        const uint64_t dmask = nb - 1;
+        for (uint32_t base = 0; base < n; base += THREADS) {
+            const uint32_t i = base + tid;
+            const uint64_t c = i < n ? buf[i] : 0ull;
+            const bool in = i < n && (pbits == 0 || (c >> (sh + w)) == prefix);
+            warp_hist_add(s.hist, static_cast<uint32_t>((c >> sh) & dmask), in);
+        }
+        __syncthreads();
+        block_rank_search<THREADS>(r, nb, s);
+        const uint32_t b = s.bc32[0], rr = s.bc32[1], cb = s.bc32[2], ab = s.bc32[3];
+        __syncthreads();
+        if (cb == 0xffffffffu) return keep_from;
+        prefix = (pbits == 0) ? b : ((prefix << w) | b);
+        pbits += w;
+        above_total += ab;
+        r = rr;
+        keep_from = prefix << sh;
+        if (above_total + cb <= slack || sh == 0) break;
+        top = sh - 1;
+    }
+    return keep_from;
 }
 
 // Exact top-k of buf[0, cnt) (unique composites): on return buf[0, min(cnt,k))
@@ -284,7 +352,10 @@ __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, ui
         // digit histogram -> exclusive offsets
         for (int i = tid; i < 256; i += THREADS) s.hist[i] = 0;
         __syncthreads();
-        for (uint32_t i = tid; i < n; i += THREADS) atomicAdd(&s.hist[(a[i] >> sh) & 0xff], 1u);
+        for (uint32_t base = 0; base < n; base += THREADS) {
+            const uint32_t i = base + tid;
+            warp_hist_add(s.hist, i < n ? static_cast<uint32_t>((a[i] >> sh) & 0xff) : 0u, i < n);
+        }
         __syncthreads();
         if (tid < 32) {
             uint32_t c[8], sum = 0;

@@ -135,34 +135,21 @@ struct FusedShared {
     uint32_t base;
     uint32_t abort;  // a bounded wait gave up: the CTA stops
     uint32_t pad2_;
+    uint32_t wc[THREADS / 32];  // per-warp region counts while gathering
     uint64_t gthr;
-    uint64_t hi;     // upper bound of the buffer's composites
 };
 
-__device__ __forceinline__ uint64_t warp_max_u64(uint64_t v) {
-#pragma unroll
-    for (int m = 16; m > 0; m >>= 1) {
-        uint64_t o = __shfl_xor_sync(kFullMask, static_cast<unsigned long long>(v), m);
-        v = o > v ? o : v;
-    }
-    return v;
-}
 
 // Appends composite c (when pass) to the shared buffer with one shared atomic
-// per warp (warp-aggregated) and keeps the buffer's upper bound.  All lanes
-// of the warp must call.
-__device__ __forceinline__ void warp_append(bool pass, uint64_t c, uint64_t* buf, uint32_t* cnt, uint64_t* hi,
-                                            uint32_t cap, uint32_t* err) {
+// per warp (warp-aggregated).  All lanes of the warp must call.
+__device__ __forceinline__ void warp_append(bool pass, uint64_t c, uint64_t* buf, uint32_t* cnt, uint32_t cap,
+                                            uint32_t* err) {
     uint32_t m = __ballot_sync(kFullMask, pass);
     if (m == 0) return;
     const uint32_t lane = lane_id();
     const uint32_t leader = __ffs(m) - 1;
-    const uint64_t mx = warp_max_u64(pass ? c : 0ull);
     uint32_t base = 0;
-    if (lane == leader) {
-        base = atomicAdd(cnt, __popc(m));
-        atomicMax(reinterpret_cast<unsigned long long*>(hi), static_cast<unsigned long long>(mx));
-    }
+    if (lane == leader) base = atomicAdd(cnt, __popc(m));
     base = __shfl_sync(kFullMask, base, leader);
     if (pass) {
         uint32_t i = base + __popc(m & lanemask_lt());
@@ -171,18 +158,39 @@ __device__ __forceinline__ void warp_append(bool pass, uint64_t c, uint64_t* buf
     }
 }
 
+// Reserves room for n entries per lane (one shared atomic per warp) and
+// returns this lane's first slot.  All lanes of the warp must call; the warp
+// total must be non-zero.
+__device__ __forceinline__ uint32_t warp_reserve(uint32_t n, uint32_t* cnt) {
+    const uint32_t incl = warp_inclusive_scan<true>(n);
+    const uint32_t total = __shfl_sync(kFullMask, incl, 31);
+    uint32_t base = 0;
+    if (lane_id() == 31) base = atomicAdd(cnt, total);
+    base = __shfl_sync(kFullMask, base, 31);
+    return base + incl - n;
+}
+
 // Write a task's output row from its m sorted output keys (low 32 bits =
 // position): value, index (automatic 1-based or custom), padding.
-template <int THREADS>
+template <int THREADS, bool kFromKey = false>
 __device__ void write_row(const FusedParams& p, const TaskView& tv, const uint64_t* sorted, uint32_t m) {
     const int tid = threadIdx.x;
+    const uint32_t nan_key = key_of_bits(tv.sp.nan_bits);
     for (uint32_t j = tid; j < tv.k; j += THREADS) {
         float v = 0.0f;
         int64_t idx = -1;
         if (j < m) {
             uint32_t pos = static_cast<uint32_t>(sorted[j]);
             if (pos >= static_cast<uint64_t>(tv.len)) pos = 0;  // bounded gather (error recorded earlier)
-            v = tv.data[pos];
+            if constexpr (kFromKey) {
+                // The value is the key's preimage unless the key is the NaN
+                // substitute's (then the element may be a NaN: read it).
+                uint32_t key = static_cast<uint32_t>(sorted[j] >> 32);
+                if (!tv.ascend) key = ~key;
+                v = (key == nan_key) ? tv.data[pos] : __uint_as_float((key & 0x80000000u) ? (key ^ 0x80000000u) : ~key);
+            } else {
+                v = tv.data[pos];
+            }
             if (tv.iin) {
                 idx = (p.idx_bytes == 8) ? static_cast<const int64_t*>(tv.iin)[pos]
                                          : static_cast<int64_t>(static_cast<const int32_t*>(tv.iin)[pos]);
@@ -201,18 +209,26 @@ __device__ void write_row(const FusedParams& p, const TaskView& tv, const uint64
 // and write the task's output row (padding slots m..k-1 with 0 / -1,
 // src/algorithm.jl:358-365).  buf has room for next_pow2(m) <= cap entries
 // and, past m, for the radix sort's shared counters.
-template <int THREADS>
+template <int THREADS, bool kFromScore = false>
 __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* buf, uint32_t m,
                             FusedShared<THREADS>& sh) {
     const int tid = threadIdx.x;
     for (uint32_t i = tid; i < m; i += THREADS) {
-        uint32_t pos = composite_pos(buf[i]);
+        const uint64_t c = buf[i];
+        uint32_t pos = composite_pos(c);
         if (pos >= static_cast<uint64_t>(tv.len)) {  // never expected; keep the gather in bounds
             record_error(p.err, kErrBounds);
             pos = 0;
         }
-        uint32_t bits = __float_as_uint(tv.data[pos]);
-        buf[i] = output_sort_key(bits, pos, tv.sp, tv.ascend);
+        if constexpr (kFromScore) {
+            // Unscaled scores are the keys of the NaN-substituted values.
+            uint32_t key = static_cast<uint32_t>(c >> 32) ^ tv.sp.flip;
+            if (!tv.ascend) key = ~key;
+            buf[i] = (static_cast<uint64_t>(key) << 32) | pos;
+        } else {
+            uint32_t bits = __float_as_uint(tv.data[pos]);
+            buf[i] = output_sort_key(bits, pos, tv.sp, tv.ascend);
+        }
     }
     __syncthreads();
     uint64_t* sorted = buf;
@@ -229,7 +245,7 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
         sorted = radix_sort_u64<THREADS>(buf, scratch, m, sh.bs, wd, db);
     }
     __syncthreads();
-    write_row<THREADS>(p, tv, sorted, m);
+    write_row<THREADS, kFromScore>(p, tv, sorted, m);
 }
 
 // Shared count, clamped to the buffer (appends past cap were dropped and
@@ -246,51 +262,31 @@ __device__ __forceinline__ uint32_t buffer_count(const FusedParams& p, FusedShar
     return cnt;
 }
 
-// Mid-stream reduction: keeps between k and max_keep entries (all of them
-// >= the returned keep_from); lo must bound every entry from below.
-// Returns keep_from, or 0 when nothing was dropped.
+// Mid-stream reduction: keeps between k and max_keep entries, all of them
+// >= the returned keep_from (0 when nothing was dropped).
 template <int THREADS>
-__device__ uint64_t shrink_mid(const FusedParams& p, uint32_t k, uint32_t max_keep, uint64_t lo, uint64_t* buf,
+__device__ uint64_t shrink_mid(const FusedParams& p, uint32_t k, uint32_t max_keep, uint64_t* buf,
                                FusedShared<THREADS>& sh) {
     const uint32_t cnt = buffer_count<THREADS>(p, sh);
+    uint64_t vor = 0, vand = ~0ull;
+    for (uint32_t i = threadIdx.x; i < cnt; i += THREADS) { uint64_t c = buf[i]; vor |= c; vand &= c; }
+    block_or_and<THREADS>(vor, vand, sh.bs);
     uint64_t kf = 0, mn = 0;
-    const uint32_t kept = block_shrink<THREADS>(buf, cnt, k, max_keep, lo, sh.hi, sh.bs, p.err, &kf, &mn);
+    const uint32_t kept = block_shrink<THREADS>(buf, cnt, k, max_keep, vand, vor, sh.bs, p.err, &kf, &mn);
     __syncthreads();
     if (threadIdx.x == 0) sh.cnt = kept;
     __syncthreads();
     return (kept >= k && kept < cnt) ? kf : 0ull;
 }
 
-// Exact top-k of a small buffer (next_pow2(cnt) <= cap and <= 4096 entries):
-// one descending bitonic sort puts the best min(cnt, k) composites first.
-// Returns their number; *kth receives the k-th composite (0 if fewer than k).
-template <int THREADS>
-__device__ uint32_t select_small(uint64_t* buf, uint32_t cnt, uint32_t k, uint64_t* kth) {
-    uint32_t P = 1;
-    while (P < cnt) P <<= 1;
-    for (uint32_t i = cnt + threadIdx.x; i < P; i += THREADS) buf[i] = 0ull;  // below every composite
-    __syncthreads();
-    bitonic_sort_u64<THREADS>(buf, P, true);
-    const uint32_t m = cnt < k ? cnt : k;
-    *kth = (m == k && m > 0) ? buf[m - 1] : 0ull;
-    return m;
-}
-
-// Exact reduction of the buffer to its best k, by bitonic sort when small,
-// else by radix selection.  Returns the number kept and the k-th composite.
+// Exact reduction of the buffer to its best k (radix selection).  Returns
+// the number kept and, through *kth, the k-th composite (0 if fewer than k).
 template <int THREADS>
 __device__ uint32_t shrink_final(const FusedParams& p, uint32_t k, uint64_t* buf, FusedShared<THREADS>& sh,
                                  uint64_t* kth) {
     const uint32_t cnt = buffer_count<THREADS>(p, sh);
-    uint32_t P = 1;
-    while (P < cnt) P <<= 1;
-    uint32_t m;
-    if (P <= kBitonicMax && P <= p.cap) {
-        m = select_small<THREADS>(buf, cnt, k, kth);
-    } else {
-        m = block_select_topk<THREADS>(buf, cnt, k, sh.bs, p.err, kth);
-        if (m < k) *kth = 0;
-    }
+    uint32_t m = block_select_topk<THREADS>(buf, cnt, k, sh.bs, p.err, kth);
+    if (m < k) *kth = 0;
     __syncthreads();
     if (threadIdx.x == 0) sh.cnt = m;
     __syncthreads();
@@ -302,7 +298,8 @@ __device__ uint32_t shrink_final(const FusedParams& p, uint32_t k, uint64_t* buf
 // of sample rank r, where r is chosen so that about 2k elements of the task
 // are expected above it.  0 (no pruning) when the sample is too small.
 template <int THREADS, bool kScale>
-__device__ uint64_t sampled_threshold(const TaskView& tv, float scaler, uint32_t k, uint64_t* buf) {
+__device__ uint64_t sampled_threshold(const TaskView& tv, float scaler, uint32_t k, uint64_t* buf,
+                                      FusedShared<THREADS>& sh, uint32_t* err) {
     constexpr uint32_t S = 1024, CH = S / 16;
     const int64_t len = tv.len;
     if (len < 8 * static_cast<int64_t>(S)) return 0ull;
@@ -310,19 +307,155 @@ __device__ uint64_t sampled_threshold(const TaskView& tv, float scaler, uint32_t
     const uint32_t r = static_cast<uint32_t>(ceilf(2.0f * lam + 4.0f * sqrtf(lam) + 12.0f));
     if (r > S / 4) return 0ull;
     const int64_t cstride = len / 16;
+    uint64_t vor = 0, vand = ~0ull;
     for (uint32_t i = threadIdx.x; i < S; i += THREADS) {
         const int64_t q = static_cast<int64_t>(i / CH) * cstride + (i % CH);
         const uint32_t bits = __float_as_uint(tv.data[q]);
-        buf[i] = make_composite(score_of<kScale>(bits, scaler, tv.sp), static_cast<uint32_t>(q));
+        const uint64_t c = make_composite(score_of<kScale>(bits, scaler, tv.sp), static_cast<uint32_t>(q));
+        buf[i] = c;
+        vor |= c;
+        vand &= c;
     }
+    block_or_and<THREADS>(vor, vand, sh.bs);  // barriers: the sample is in buf
+    const uint64_t kf = block_rank_threshold<THREADS>(buf, S, r, 4 * r, vand, vor, sh.bs);
     __syncthreads();
-    bitonic_sort_u64<THREADS>(buf, S, true);
-    const uint64_t c = buf[r - 1];
+    return kf > 0 ? kf - 1 : 0ull;
+}
+
+// Candidate appends go to one region per warp (kRegionEntries in total, after
+// the settled region of the shared buffer) so that a warp counts its own
+// entries in a register.  gather_regions moves every warp's entries behind the
+// settled ones, leaving the candidates in [0, sh.cnt); all threads must call.
+constexpr uint32_t kRegionEntries = 2048;
+
+template <int THREADS, uint32_t R>
+__device__ void gather_regions(uint64_t* s_buf, uint32_t cap_s, uint32_t& wcnt, FusedShared<THREADS>& sh) {
+    constexpr int NW = THREADS / 32;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t wc = wcnt < R ? wcnt : R;
+    if (lane == 0) sh.wc[warp] = wc;
     __syncthreads();
-    return c - 1;
+    uint32_t off = sh.cnt, total = sh.cnt;
+#pragma unroll
+    for (int i = 0; i < NW; ++i) {
+        off += (i < warp) ? sh.wc[i] : 0u;
+        total += sh.wc[i];
+    }
+    // Warps move their entries one after another: warp w's destination ends
+    // at or before warp w+1's region, so no entry is overwritten unread.
+    for (int ww = 0; ww < NW; ++ww) {
+        if (sh.wc[ww] == 0) continue;  // same decision in every thread
+        if (warp == ww && off != cap_s + ww * R) {
+            const uint64_t* region = s_buf + cap_s + ww * R;
+            for (uint32_t base = 0; base < wc; base += 32) {
+                const uint32_t idx = base + lane;
+                const uint64_t x = idx < wc ? region[idx] : 0ull;
+                __syncwarp();
+                if (idx < wc) s_buf[off + idx] = x;
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sh.cnt = total;
+    __syncthreads();
+    wcnt = 0;
+}
+
+// Cheap superset test of "composite > thr" on raw float values.  An element
+// whose composite exceeds thr has a score >= thr's score; in value terms that
+// is x >= t (largest) or x <= t (smallest) for the value t whose key is that
+// score, and a float compare accepts at least those values (it only adds
+// +-0 ties, which the exact test on candidates settles).  NaN elements score
+// as the reference's substitute, so they may pass only when that substitute
+// does (nan_pass).  Values are compared sign-flipped for the smallest, so
+// one compare covers both directions.
+struct FastFilter {
+    float t;          // compare x * dir >= t (after the sign flip)
+    float tr;         // the same threshold unflipped: x <= tr (smallest)
+    uint32_t dir;     // 0 (largest) or 0x80000000 (smallest): sign flip of x
+    bool nan_pass;
+    float4 pad4;      // value that never passes (fills past the end of a segment)
+};
+
+__device__ __forceinline__ float value_of_key(uint32_t key) {
+    return __uint_as_float((key & 0x80000000u) ? (key ^ 0x80000000u) : ~key);
+}
+
+template <bool kScale>
+__device__ __forceinline__ FastFilter make_fast_filter(uint64_t thr, const ScoreParams& sp, float scaler) {
+    constexpr uint32_t kNegInf = 0x007fffffu, kPosInf = 0xff800000u;  // keys of -inf, +inf
+    FastFilter f;
+    const uint32_t s = static_cast<uint32_t>(thr >> 32);
+    const bool largest = sp.flip == 0;
+    f.dir = largest ? 0u : 0x80000000u;
+    float t;
+    if (largest) {  // pass iff key >= s
+        t = (s <= kNegInf) ? -INFINITY : (s > kPosInf ? __uint_as_float(0x7fc00000u) : value_of_key(s));
+    } else {        // pass iff key <= ~s
+        const uint32_t K = ~s;
+        t = (K >= kPosInf) ? INFINITY : (K < kNegInf ? __uint_as_float(0x7fc00000u) : value_of_key(K));
+    }
+    f.t = __uint_as_float(__float_as_uint(t) ^ f.dir);
+    f.tr = t;
+    const float never = largest ? -INFINITY : INFINITY;  // fails unless everything passes
+    f.pad4 = make_float4(never, never, never, never);
+    uint32_t nan_score = sp.nan_score;
+    if constexpr (kScale)
+        nan_score = key_of_bits(__float_as_uint(__fsub_rn(__uint_as_float(sp.nan_bits), scaler))) ^ sp.flip;
+    f.nan_pass = nan_score >= s;
+    return f;
 }
 
 constexpr uint32_t kWaitPolls = 1u << 22;
+
+// Geometry of one work item, identical in every thread of the CTA.
+struct SegGeom {
+    FusedSeg sg;
+    FusedTask td;
+    int64_t s0, s1, a0, a1, nvec;
+    uint32_t ntiles;
+    bool skip;  // retry launch and the task was not flagged
+};
+
+template <int TILE, bool kScale>
+__device__ __forceinline__ SegGeom seg_geom(const FusedParams& p, int w, TaskView* tv) {
+    SegGeom g;
+    g.sg = p.segs[w];
+    g.td = p.tasks[g.sg.task];
+    g.skip = p.retry && p.fail[g.sg.task] == 0;
+    *tv = task_view<kScale>(p, g.sg.task, g.td);
+    g.s0 = g.sg.pos;
+    g.s1 = static_cast<int64_t>(g.sg.pos) + g.sg.len;
+    // Position q sits on a 16-byte boundary iff (q + mis) % 4 == 0.
+    const int64_t mis = static_cast<int64_t>((reinterpret_cast<uintptr_t>(tv->data) >> 2) & 3);
+    g.a0 = ((g.s0 + mis + 3) & ~int64_t(3)) - mis;
+    g.a1 = ((g.s1 + mis) & ~int64_t(3)) - mis;
+    if (g.a0 > g.a1) { g.a0 = g.s1; g.a1 = g.s1; }  // no aligned body: everything is head
+    g.nvec = (g.a1 - g.a0) >> 2;
+    g.ntiles = static_cast<uint32_t>((g.nvec * 4 + TILE - 1) / TILE);
+    return g;
+}
+
+// Thread 0: start the bulk copy of tile i of a segment into ring stage
+// (first + i) % STAGES.
+template <int TILE, int STAGES>
+__device__ __forceinline__ void issue_tile(float* ring, uint64_t* bars, const TaskView& tv, const SegGeom& g,
+                                           uint32_t i, uint32_t first) {
+    const uint32_t st = (first + i) % STAGES;
+    const int64_t e0 = static_cast<int64_t>(i) * TILE;
+    const uint32_t bytes = static_cast<uint32_t>(min(static_cast<int64_t>(TILE), g.nvec * 4 - e0)) * 4u;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bars + st, bytes);
+    bulk_load(ring + static_cast<size_t>(st) * TILE, tv.data + g.a0 + e0, bytes, bars + st);
+}
+
+template <int TILE, int STAGES>
+__device__ __forceinline__ void issue_prologue(float* ring, uint64_t* bars, const TaskView& tv, const SegGeom& g,
+                                               uint32_t first) {
+    for (uint32_t i = 0; i < g.ntiles && i < static_cast<uint32_t>(STAGES); ++i)
+        issue_tile<TILE, STAGES>(ring, bars, tv, g, i, first);
+}
 
 template <int THREADS, int VEC, int STAGES, bool kScale>
 __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_kernel(FusedParams p) {
@@ -330,49 +463,55 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
     __shared__ FusedShared<THREADS> sh;
     constexpr int U = VEC / 4;                      // float4 per thread per tile
     constexpr uint32_t TILE = THREADS * VEC;        // elements per tile (one ring stage)
+    constexpr int NW = THREADS / 32;
+    constexpr uint32_t R = kRegionEntries / NW;     // append region of each warp
+    constexpr uint32_t RSLACK = 2 * U * 4;           // refill the regions before they run short
     float* ring = reinterpret_cast<float*>(smem_raw);
     uint64_t* s_buf = reinterpret_cast<uint64_t*>(smem_raw + static_cast<size_t>(STAGES) * TILE * 4);
     uint64_t* bars = s_buf + p.cap;
     const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const uint32_t lt = lanemask_lt();
     const uint32_t cap = p.cap;
-    const uint32_t compact_at = cap - TILE - 8;     // host guarantees cap >= kmax + TILE + headroom
+    const uint32_t cap_s = p.cap - kRegionEntries;  // settled region [0, cap_s), then the warp regions
+    uint64_t* region = s_buf + cap_s + warp * R;
+    // Merge path (contiguous buffer): shrink once fewer than this many slots are free.
+    const uint32_t compact_at = cap - max(cap / 8, static_cast<uint32_t>(THREADS) + 8u);
 
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) mbar_init(bars + s, 1);
         fence_mbar_init();
         sh.abort = 0;
+        sh.work = static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
     }
     __syncthreads();
-    uint32_t gtile = 0;  // tiles this CTA consumed so far: ring stage and mbarrier phase
+    uint32_t gtile = 0;      // tiles this CTA consumed so far: ring stage and mbarrier phase
+    int w = sh.work;
+    bool prefetched = false;  // the current item's first tiles are already in flight
 
-    for (;;) {
-        if (tid == 0) sh.work = static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
-        __syncthreads();
-        const int w = sh.work;
-        if (w >= p.nsegs || sh.abort) break;
-        const FusedSeg sg = p.segs[w];
-        const int t = sg.task;
-        if (p.retry && p.fail[t] == 0) {  // retry launch: only flagged tasks
+    while (w < p.nsegs) {
+        TaskView tv;
+        const SegGeom G = seg_geom<TILE, kScale>(p, w, &tv);
+        const int t = G.sg.task;
+        int nw = p.nsegs;  // next work item, fetched once this one's tiles are consumed
+        if (G.skip) {      // retry launch: only flagged tasks run
             __syncthreads();
+            if (tid == 0) sh.work = static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
+            __syncthreads();
+            w = sh.work;
+            prefetched = false;
             continue;
         }
-        const FusedTask td = p.tasks[t];
-        const TaskView tv = task_view<kScale>(p, t, td);
+        const FusedTask& td = G.td;
         const uint32_t k = tv.k;
-        const uint32_t mid_keep = k + (cap - k - TILE) / 4;
+        const uint32_t mid_keep = k + (cap_s - k) / 2;
         const bool multi = td.nseg > 1;
         const float scaler = kScale ? task_scaler(tv.data, 0, tv.len, 1) : 0.0f;
-        const int64_t s0 = sg.pos, s1 = static_cast<int64_t>(sg.pos) + sg.len;
-        // Position q sits on a 16-byte boundary iff (q + mis) % 4 == 0.
-        const int64_t mis = static_cast<int64_t>((reinterpret_cast<uintptr_t>(tv.data) >> 2) & 3);
-        int64_t a0 = ((s0 + mis + 3) & ~int64_t(3)) - mis;
-        int64_t a1 = ((s1 + mis) & ~int64_t(3)) - mis;
-        if (a0 > a1) { a0 = s1; a1 = s1; }   // no aligned body: everything is head
-        const int64_t nvec = (a1 - a0) >> 2;
-        const uint32_t ntiles = static_cast<uint32_t>((nvec * 4 + TILE - 1) / TILE);
+        bool next_prefetched = false;
 
-        bool done_task = false;
-        for (int attempt = 0; attempt < 2 && !done_task; ++attempt) {
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            if (!prefetched && tid == 0) issue_prologue<TILE, STAGES>(ring, bars, tv, G, gtile);
+            prefetched = false;
             uint64_t thr = 0;
             bool sampled_local = false;
             if (multi) {
@@ -380,211 +519,301 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                 __syncthreads();
                 thr = sh.gthr;
             } else if (attempt == 0) {
-                thr = sampled_threshold<THREADS, kScale>(tv, scaler, k, s_buf);
+                // Overlaps with the tile copies already in flight.
+                thr = sampled_threshold<THREADS, kScale>(tv, scaler, k, s_buf, sh, p.err);
                 sampled_local = thr != 0;
             }
-            if (tid == 0) { sh.cnt = 0; sh.hi = 0; sh.gthr = thr; }
             __syncthreads();
-            uint64_t lo = thr;  // every buffered composite is >= lo
+            if (tid == 0) { sh.cnt = 0; sh.gthr = thr; }
+            __syncthreads();
+            uint32_t wcnt = 0;  // entries in this warp's region (same in all its lanes)
 
-            // Prologue: start the first STAGES tile copies.
-            if (tid == 0) {
-                for (uint32_t i = 0; i < ntiles && i < static_cast<uint32_t>(STAGES); ++i) {
-                    const uint32_t st = (gtile + i) % STAGES;
-                    const int64_t e0 = static_cast<int64_t>(i) * TILE;
-                    const uint32_t bytes = static_cast<uint32_t>(min(static_cast<int64_t>(TILE), nvec * 4 - e0)) * 4u;
-                    fence_proxy_async_smem();
-                    mbar_arrive_expect_tx(bars + st, bytes);
-                    bulk_load(ring + static_cast<size_t>(st) * TILE, tv.data + a0 + e0, bytes, bars + st);
-                }
-            }
-            // Head [s0, a0) and tail [a1, s1): fewer than 4 elements each.
-            if (tid < 32) {
-                const int nh = static_cast<int>(a0 - s0), nt = static_cast<int>(s1 - a1);
+            // Head [s0, a0) and tail [a1, s1): fewer than 4 elements each (warp 0).
+            if (warp == 0) {
+                const int nh = static_cast<int>(G.a0 - G.s0), nt = static_cast<int>(G.s1 - G.a1);
                 bool pass = false;
                 uint64_t c = 0;
                 int64_t q = -1;
-                if (tid < nh) q = s0 + tid;
-                else if (tid >= 8 && tid - 8 < nt) q = a1 + (tid - 8);
+                if (tid < nh) q = G.s0 + tid;
+                else if (tid >= 8 && tid - 8 < nt) q = G.a1 + (tid - 8);
                 if (q >= 0) {
                     uint32_t bits = __float_as_uint(tv.data[q]);
                     c = make_composite(score_of<kScale>(bits, scaler, tv.sp), static_cast<uint32_t>(q));
                     pass = c > thr;
                 }
-                warp_append(pass, c, s_buf, &sh.cnt, &sh.hi, cap, p.err);
+                const uint32_t m = __ballot_sync(kFullMask, pass);
+                if (pass) region[__popc(m & lt)] = c;
+                wcnt = __popc(m);
             }
-            const uint32_t pos0 = static_cast<uint32_t>(a0);
+            const uint32_t pos0 = static_cast<uint32_t>(G.a0);
+            FastFilter ff = make_fast_filter<kScale>(thr, tv.sp, scaler);
+            const int64_t nvec = G.nvec;
+            const uint32_t ntiles = G.ntiles;
+            uint64_t gnext = 0;  // thread 0: latest global threshold, read a few tiles ahead
             for (uint32_t it = 0; it < ntiles; ++it) {
                 const uint32_t g = gtile + it;
                 const uint32_t st = g % STAGES;
+                bool flag = false;  // this thread needs the slow path after the tile
                 if (!mbar_wait_bounded(bars + st, (g / STAGES) & 1u, kWaitPolls)) {
                     record_error(p.err, kErrTimeout);
                     sh.abort = 1;
+                    flag = true;
                 }
+                if (multi && tid == 0 && (it & 7) == 0) gnext = load_volatile_u64(p.gthr + t);
                 const float4* t4 = reinterpret_cast<const float4*>(ring + static_cast<size_t>(st) * TILE);
                 const int64_t qb = static_cast<int64_t>(it) * (TILE / 4);
+                // Fast superset filter: one compare per element, and only
+                // "does any element of this thread pass" is kept.
                 float4 v[U];
-                uint32_t pm = 0;
+                const bool full = qb + static_cast<int64_t>(U) * THREADS <= nvec;
+                bool anyp = false;
+                if (full) {
 #pragma unroll
-                for (int j = 0; j < U; ++j) {
-                    const int64_t q = qb + j * THREADS + tid;
-                    v[j] = (q < nvec) ? t4[j * THREADS + tid] : make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (q < nvec) {
-                        const uint32_t pb = pos0 + static_cast<uint32_t>(q) * 4u;
-                        const float f[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            uint64_t c = make_composite(score_of<kScale>(__float_as_uint(f[e]), scaler, tv.sp), pb + e);
-                            pm |= (c > thr) ? (1u << (j * 4 + e)) : 0u;
-                        }
-                    }
-                }
-                if (__any_sync(kFullMask, pm != 0)) {
+                    for (int j = 0; j < U; ++j) v[j] = t4[j * THREADS + tid];
+                } else {
 #pragma unroll
                     for (int j = 0; j < U; ++j) {
                         const int64_t q = qb + j * THREADS + tid;
-                        const uint32_t pb = pos0 + static_cast<uint32_t>(q) * 4u;
-                        const float f[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+                        v[j] = (q < nvec) ? t4[j * THREADS + tid] : ff.pad4;
+                    }
+                }
+                if constexpr (kScale) {
 #pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const bool ps = (pm >> (j * 4 + e)) & 1u;
-                            uint64_t c = ps ? make_composite(score_of<kScale>(__float_as_uint(f[e]), scaler, tv.sp), pb + e)
-                                            : 0ull;
-                            warp_append(ps, c, s_buf, &sh.cnt, &sh.hi, cap, p.err);
+                    for (int j = 0; j < U; ++j) {
+                        v[j].x = __fsub_rn(v[j].x, scaler); v[j].y = __fsub_rn(v[j].y, scaler);
+                        v[j].z = __fsub_rn(v[j].z, scaler); v[j].w = __fsub_rn(v[j].w, scaler);
+                    }
+                }
+                if (ff.dir == 0u && !ff.nan_pass) {
+#pragma unroll
+                    for (int j = 0; j < U; ++j)
+                        anyp |= (v[j].x >= ff.t) | (v[j].y >= ff.t) | (v[j].z >= ff.t) | (v[j].w >= ff.t);
+                } else if (!ff.nan_pass) {
+#pragma unroll
+                    for (int j = 0; j < U; ++j)
+                        anyp |= (v[j].x <= ff.tr) | (v[j].y <= ff.tr) | (v[j].z <= ff.tr) | (v[j].w <= ff.tr);
+                } else if (ff.dir == 0u) {
+#pragma unroll
+                    for (int j = 0; j < U; ++j)
+                        anyp |= !(v[j].x < ff.t) | !(v[j].y < ff.t) | !(v[j].z < ff.t) | !(v[j].w < ff.t);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < U; ++j)
+                        anyp |= !(v[j].x > ff.tr) | !(v[j].y > ff.tr) | !(v[j].z > ff.tr) | !(v[j].w > ff.tr);
+                }
+                // Candidates (a superset of the passing elements, kept with
+                // their exact composites) go to this warp's region: one warp
+                // scan of the per-lane counts, then each lane writes its own.
+                uint32_t dm = 0;  // candidates that found no room (re-offered after a shrink)
+                if (__any_sync(kFullMask, anyp)) {
+                    uint32_t pm = 0;
+                    if (anyp) {
+#pragma unroll
+                        for (int j = 0; j < U; ++j) {
+                            const int64_t q = qb + j * THREADS + tid;
+                            const float f4[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const float x = __uint_as_float(__float_as_uint(f4[e]) ^ ff.dir);
+                                const bool ps = (q < nvec) && (ff.nan_pass ? !(x < ff.t) : (x >= ff.t));
+                                pm |= static_cast<uint32_t>(ps) << (j * 4 + e);
+                            }
                         }
                     }
-                }
-                uint64_t gnew = 0;
-                if (multi && tid == 0 && (it & 7) == 7) gnew = load_volatile_u64(p.gthr + t);
-                if (multi && tid == 0 && gnew > sh.gthr) sh.gthr = gnew;
-                // Snapshot shared state between two barriers: nobody may read
-                // it after a faster thread started on the next tile.
-                __syncthreads();
-                const uint32_t cnt_now = sh.cnt;
-                const uint64_t g_now = sh.gthr;
-                const uint32_t ab = sh.abort;
-                __syncthreads();
-                if (ab) {
-                    // Drain the copies this CTA still has in flight (bounded).
-                    if (tid == 0) {
-                        for (uint32_t i = it + 1; i < ntiles && i < it + STAGES; ++i)
-                            mbar_wait_bounded(bars + (gtile + i) % STAGES, ((gtile + i) / STAGES) & 1u, kWaitPolls);
+                    const uint32_t n = __popc(pm);
+                    const uint32_t incl = warp_inclusive_scan<true>(n);
+                    uint32_t slot = wcnt + incl - n;
+                    wcnt += __shfl_sync(kFullMask, incl, 31);
+                    const float* tile = ring + static_cast<size_t>(st) * TILE;
+                    for (uint32_t m = pm; m; m &= m - 1) {
+                        const int b = __ffs(m) - 1;
+                        const uint32_t li = static_cast<uint32_t>((b >> 2) * THREADS + tid) * 4u + (b & 3);
+                        const uint32_t pos = pos0 + static_cast<uint32_t>(qb) * 4u + li;
+                        const uint64_t c = make_composite(score_of<kScale>(__float_as_uint(tile[li]), scaler, tv.sp), pos);
+                        if (slot < R) region[slot] = c;
+                        else dm |= 1u << b;
+                        ++slot;
                     }
-                    __syncthreads();
-                    return;
+                    flag = flag || dm != 0 || wcnt + RSLACK > R;
+                }
+                const bool refresh = multi && (it & 7) == 7;
+                if (refresh && tid == 0 && gnext > sh.gthr) sh.gthr = gnext;
+                // One barrier per tile; it also tells every thread whether a
+                // warp region runs short, candidates wait for room, or a wait
+                // timed out.
+                if (__syncthreads_or(flag ? 1 : 0)) {
+                    if (sh.abort) {
+                        // Drain the copies this CTA still has in flight (bounded).
+                        if (tid == 0) {
+                            for (uint32_t i = it + 1; i < ntiles && i < it + STAGES; ++i)
+                                mbar_wait_bounded(bars + (gtile + i) % STAGES, ((gtile + i) / STAGES) & 1u,
+                                                  kWaitPolls);
+                        }
+                        __syncthreads();
+                        return;
+                    }
+                    // Gather the regions, shrink, raise the threshold, and
+                    // re-offer the candidates that found no room; repeat until
+                    // all of them are placed or no longer pass.
+                    for (int round = 0; round < 16; ++round) {
+                        gather_regions<THREADS, R>(s_buf, cap_s, wcnt, sh);
+                        const uint64_t kf = shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh);
+                        if (kf != 0) {
+                            thr = (kf - 1) > thr ? (kf - 1) : thr;
+                            ff = make_fast_filter<kScale>(thr, tv.sp, scaler);
+                            if (multi && tid == 0)
+                                atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), kf - 1);
+                        }
+                        const uint32_t rm_in = dm;
+                        dm = 0;
+                        bool again = false;
+                        if (__any_sync(kFullMask, rm_in != 0)) {
+                            const float* tile = ring + static_cast<size_t>(st) * TILE;
+                            uint32_t rm = 0;
+                            for (uint32_t m = rm_in; m; m &= m - 1) {
+                                const int b = __ffs(m) - 1;
+                                const uint32_t li = static_cast<uint32_t>((b >> 2) * THREADS + tid) * 4u + (b & 3);
+                                const uint32_t pos = pos0 + static_cast<uint32_t>(qb) * 4u + li;
+                                const uint64_t c =
+                                    make_composite(score_of<kScale>(__float_as_uint(tile[li]), scaler, tv.sp), pos);
+                                rm |= (c > thr) ? (1u << b) : 0u;
+                            }
+                            const uint32_t n = __popc(rm);
+                            const uint32_t incl = warp_inclusive_scan<true>(n);
+                            uint32_t slot = wcnt + incl - n;
+                            wcnt += __shfl_sync(kFullMask, incl, 31);
+                            for (uint32_t m = rm; m; m &= m - 1) {
+                                const int b = __ffs(m) - 1;
+                                const uint32_t li = static_cast<uint32_t>((b >> 2) * THREADS + tid) * 4u + (b & 3);
+                                const uint32_t pos = pos0 + static_cast<uint32_t>(qb) * 4u + li;
+                                const uint64_t c =
+                                    make_composite(score_of<kScale>(__float_as_uint(tile[li]), scaler, tv.sp), pos);
+                                if (slot < R) region[slot] = c;
+                                else dm |= 1u << b;
+                                ++slot;
+                            }
+                            again = dm != 0 || wcnt + RSLACK > R;
+                        }
+                        if (!__syncthreads_or(again ? 1 : 0)) break;
+                    }
+                    if (dm != 0) record_error(p.err, kErrCapacity);
+                }
+                if (refresh) {
+                    const uint64_t g_now = sh.gthr;
+                    if (g_now > thr) {
+                        thr = g_now;
+                        ff = make_fast_filter<kScale>(thr, tv.sp, scaler);
+                    }
                 }
                 // The stage just read is free: refill it with tile it + STAGES.
-                if (tid == 0 && it + STAGES < ntiles) {
-                    const int64_t e0 = static_cast<int64_t>(it + STAGES) * TILE;
-                    const uint32_t bytes = static_cast<uint32_t>(min(static_cast<int64_t>(TILE), nvec * 4 - e0)) * 4u;
-                    fence_proxy_async_smem();
-                    mbar_arrive_expect_tx(bars + st, bytes);
-                    bulk_load(ring + static_cast<size_t>(st) * TILE, tv.data + a0 + e0, bytes, bars + st);
-                }
-                if (cnt_now > compact_at) {
-                    const uint64_t kf = shrink_mid<THREADS>(p, k, mid_keep, lo, s_buf, sh);
-                    if (kf != 0) {
-                        lo = kf;
-                        thr = (kf - 1) > thr ? (kf - 1) : thr;
-                        if (multi && tid == 0) atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), kf - 1);
-                    }
-                }
-                if (multi) thr = g_now > thr ? g_now : thr;
+                if (tid == 0 && it + STAGES < ntiles) issue_tile<TILE, STAGES>(ring, bars, tv, G, it + STAGES, gtile);
             }
             gtile += ntiles;
-            __syncthreads();
+            gather_regions<THREADS, R>(s_buf, cap_s, wcnt, sh);  // all candidates now in [0, sh.cnt)
 
             if (!multi) {
-                uint64_t kth = 0;
                 const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
-                const uint32_t have = buffer_count<THREADS>(p, sh);
-                if (have < want && sampled_local) continue;  // sample overestimated: redo without it
-                const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh, &kth);
-                if (m != want && tid == 0) record_error(p.err, kErrInternal);
-                finish_task<THREADS>(p, tv, s_buf, m < want ? m : want, sh);
+                if (sh.cnt < want && sampled_local) continue;  // sample overestimated: redo without it
             }
-            done_task = true;
+            break;
         }
-        if (!multi) continue;
 
-        // Multi-segment task: publish this segment's k-th composite, append the
-        // survivors to the task's candidate region, count the segment done.
-        uint64_t kth = 0;
-        shrink_final<THREADS>(p, k, s_buf, sh, &kth);
-        if (tid == 0) {
-            if (kth != 0) atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), kth - 1);
-            sh.gthr = load_volatile_u64(p.gthr + t);
-        }
+        // This item's tiles are all consumed: fetch the next item and start its
+        // first tile copies, so they overlap the selection work below.
+        if (tid == 0) sh.work = static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
         __syncthreads();
-        {
-            const uint64_t g = sh.gthr;
-            const uint32_t cnt = sh.cnt;
-            uint64_t* dst = p.cand + td.cbase;
-            const uint32_t region = static_cast<uint32_t>(td.nseg) * p.kmax;
-            for (uint32_t b0 = 0; b0 < cnt; b0 += THREADS) {
-                uint32_t i = b0 + tid;
-                uint64_t c = (i < cnt) ? s_buf[i] : 0ull;
-                bool keep = (i < cnt) && c > g;
-                uint32_t total;
-                uint32_t off = block_exclusive_scan<THREADS>(keep ? 1u : 0u, &total, sh.bs);
-                if (tid == 0 && total) sh.base = atomicAdd(p.task_cnt + t, total);
-                __syncthreads();
-                if (keep) {
-                    uint32_t o = sh.base + off;
-                    if (o < region) dst[o] = c;
-                    else record_error(p.err, kErrCapacity);
+        nw = sh.work;
+        if (nw < p.nsegs) {
+            TaskView ntv;
+            const SegGeom NG = seg_geom<TILE, kScale>(p, nw, &ntv);
+            if (!NG.skip) {
+                if (tid == 0) issue_prologue<TILE, STAGES>(ring, bars, ntv, NG, gtile);
+                next_prefetched = true;
+            }
+        }
+
+        if (!multi) {
+            uint64_t kth = 0;
+            const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
+            const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh, &kth);
+            if (m != want && tid == 0) record_error(p.err, kErrInternal);
+            finish_task<THREADS, !kScale>(p, tv, s_buf, m < want ? m : want, sh);
+        } else {
+            // Multi-segment task: publish this segment's k-th composite, append
+            // the survivors to the task's candidate region, count the segment.
+            uint64_t kth = 0;
+            shrink_final<THREADS>(p, k, s_buf, sh, &kth);
+            if (tid == 0) {
+                if (kth != 0) atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), kth - 1);
+                sh.gthr = load_volatile_u64(p.gthr + t);
+            }
+            __syncthreads();
+            {
+                const uint64_t g = sh.gthr;
+                const uint32_t cnt = sh.cnt;
+                uint64_t* dst = p.cand + td.cbase;
+                const uint32_t region = static_cast<uint32_t>(td.nseg) * p.kmax;
+                for (uint32_t b0 = 0; b0 < cnt; b0 += THREADS) {
+                    uint32_t i = b0 + tid;
+                    uint64_t c = (i < cnt) ? s_buf[i] : 0ull;
+                    bool keep = (i < cnt) && c > g;
+                    uint32_t total;
+                    uint32_t off = block_exclusive_scan<THREADS>(keep ? 1u : 0u, &total, sh.bs);
+                    if (tid == 0 && total) sh.base = atomicAdd(p.task_cnt + t, total);
+                    __syncthreads();
+                    if (keep) {
+                        uint32_t o = sh.base + off;
+                        if (o < region) dst[o] = c;
+                        else record_error(p.err, kErrCapacity);
+                    }
+                    __syncthreads();
+                }
+            }
+            __threadfence();
+            __syncthreads();
+            if (tid == 0) {
+                uint32_t done = atomicAdd(p.task_done + t, 1u);
+                sh.last = (done == static_cast<uint32_t>(td.nseg - 1)) ? 1u : 0u;
+            }
+            __syncthreads();
+            if (sh.last) {
+                // Last segment of the task: merge all segments' survivors.
+                __threadfence();
+                if (tid == 0) {
+                    sh.cnt = 0;
+                    sh.gthr = load_volatile_u64(p.gthr + t);
+                    sh.base = __ldcg(p.task_cnt + t);
                 }
                 __syncthreads();
-            }
-        }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) {
-            uint32_t done = atomicAdd(p.task_done + t, 1u);
-            sh.last = (done == static_cast<uint32_t>(td.nseg - 1)) ? 1u : 0u;
-        }
-        __syncthreads();
-        if (!sh.last) continue;
-
-        // Last segment of the task: merge all segments' survivors.
-        __threadfence();
-        if (tid == 0) {
-            sh.cnt = 0;
-            sh.hi = 0;
-            sh.gthr = load_volatile_u64(p.gthr + t);
-            sh.base = __ldcg(p.task_cnt + t);
-        }
-        __syncthreads();
-        const uint64_t g = sh.gthr;
-        const uint32_t region = static_cast<uint32_t>(td.nseg) * p.kmax;
-        const uint32_t n = sh.base < region ? sh.base : region;
-        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
-        uint64_t mlo = g;
-        for (uint32_t b0 = 0; b0 < n; b0 += 4 * THREADS) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                uint32_t i = b0 + j * THREADS + tid;
-                uint64_t c = (i < n) ? __ldcg(src + i) : 0ull;
-                warp_append((i < n) && c > g, c, s_buf, &sh.cnt, &sh.hi, cap, p.err);
-            }
-            __syncthreads();
-            const uint32_t cnt_now = sh.cnt;
-            __syncthreads();
-            if (cnt_now > compact_at) {
-                const uint64_t kf = shrink_mid<THREADS>(p, k, mid_keep, mlo, s_buf, sh);
-                if (kf != 0) mlo = kf;
+                const uint64_t g = sh.gthr;
+                const uint32_t region = static_cast<uint32_t>(td.nseg) * p.kmax;
+                const uint32_t n = sh.base < region ? sh.base : region;
+                const unsigned long long* src = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
+                for (uint32_t b0 = 0; b0 < n; b0 += THREADS) {
+                    {
+                        uint32_t i = b0 + tid;
+                        uint64_t c = (i < n) ? __ldcg(src + i) : 0ull;
+                        warp_append((i < n) && c > g, c, s_buf, &sh.cnt, cap, p.err);
+                    }
+                    __syncthreads();
+                    const uint32_t cnt_now = sh.cnt;
+                    __syncthreads();
+                    if (cnt_now > compact_at) shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh);
+                }
+                __syncthreads();
+                const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh, &kth);
+                if (m < k && (td.flags & kTaskSampled) && !p.retry) {
+                    // The sampled threshold was above the task's k-th composite.
+                    if (tid == 0) p.fail[t] = 1u;
+                } else {
+                    if (m != k && tid == 0) record_error(p.err, kErrInternal);
+                    finish_task<THREADS, !kScale>(p, tv, s_buf, m < k ? m : k, sh);
+                }
             }
         }
         __syncthreads();
-        const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh, &kth);
-        if (m < k && (td.flags & kTaskSampled) && !p.retry) {
-            // The sampled threshold was above the task's k-th composite.
-            if (tid == 0) p.fail[t] = 1u;
-            __syncthreads();
-            continue;
-        }
-        if (m != k && tid == 0) record_error(p.err, kErrInternal);
-        finish_task<THREADS>(p, tv, s_buf, m < k ? m : k, sh);
+        w = nw;
+        prefetched = next_prefetched;
     }
 }
 
