@@ -97,6 +97,30 @@ int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const floa
                     const void* h_indices, int64_t indices_len, const int64_t* h_task_lens, int64_t num_tasks,
                     int64_t k, int largest, int rev, radik_ws* ws, void* stream);
 
+/* No counterpart in the reference (RadiK.jl always allocates a workspace).
+ * Same arguments and results as radik_topk_radix_select without a workspace:
+ * the fused kernel's scratch lives in one static 8 MiB device array per
+ * device, so the call performs no device allocation or free.  It serves
+ * callers that must not allocate device memory where they call: a memory
+ * pool's out-of-memory handler or allocator callback, a process under a hard
+ * device-memory cap, or a loop that cannot take cudaMalloc's implicit device
+ * synchronisation.
+ * Limits: k <= 4096, and the batch's scratch (about 40 bytes per task, 16
+ * per segment, k * 8 bytes per segment of a task split across several
+ * blocks) must fit in 8 MiB; larger calls fail with RADIK_ERR_WS_TOO_SMALL
+ * and a message giving the bytes needed.  RADIK_PLAIN and RADIK_ASYNC are
+ * rejected: the call clears the scratch state that must start at zero,
+ * uploads the plan, launches, and waits for `stream` before returning.
+ * The first call on each device does set-up (cudaGetSymbolAddress of the
+ * static array, kernel attributes); make it before any stream capture.  A
+ * capturing stream is rejected with RADIK_ERR_CAPTURE.
+ * All calls on one device share the array: calls that overlap in time (from
+ * several host threads, or on streams that are not ordered with each other)
+ * race and corrupt each other's results. */
+int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_val_in,
+                       const void* d_idx_in, const int64_t* h_task_lens, int64_t num_tasks, int64_t k,
+                       uint32_t flags, void* stream);
+
 /* ---- Stage entry points: the reference kernels' own contracts ----------- */
 
 /* count_bin_ex_kernel!, src/kernels/count_bin.jl:78-203: per-task histogram

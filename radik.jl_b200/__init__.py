@@ -180,6 +180,33 @@ def topk_radix_select_(val_out, idx_out, ws: RadiKWorkspace, val_in, idx_in, tas
     return val_out, idx_out
 
 
+def topk_radix_select_noalloc_(val_out, idx_out, val_in, idx_in, task_lens, k: int, largest: bool = True,
+                               ascend: bool = True, withscale: bool = False, withidxin: bool = False,
+                               *, stream=None):
+    """``topk_radix_select_`` without a workspace (no counterpart in the
+    reference): the engine's scratch is a static 8 MiB device array, so the
+    call allocates no device memory -- for callers inside a memory pool's
+    out-of-memory path or under a hard memory cap.  k <= 4096 and the batch's
+    scratch must fit in 8 MiB, else RadiKError.  Calls that overlap in time
+    on one device race; the first call on a device does set-up and must come
+    before any stream capture."""
+    _check_cuda(val_out, "val_out")
+    _check_cuda(idx_out, "idx_out")
+    _check_cuda(val_in, "val_in")
+    _check_float32(val_in)
+    if withidxin:
+        _check_cuda(idx_in, "idx_in")
+        if idx_in.dtype != idx_out.dtype:
+            raise RadiKError("idx_in and idx_out must have the same element type")
+    lens = _lens_array(task_lens)
+    L = load()
+    flags = _flags(largest, ascend, withscale, withidxin)
+    check(L.radik_topk_noalloc(_ptr(val_out), _ptr(idx_out), _idx_bytes(idx_out.dtype), _ptr(val_in),
+                               _ptr(idx_in) if withidxin else None, lens.ctypes.data_as(ctypes.c_void_p),
+                               len(lens), int(k), flags, _stream(stream)))
+    return val_out, idx_out
+
+
 def _split_args(task_lens_or_k, k, data):
     if k is None:
         return [int(data.numel())], int(task_lens_or_k), True

@@ -29,7 +29,7 @@ STATUS = {
 # Every symbol include/radik.h declares (checked by the CPU test suite).
 EXPORTS = (
     "radik_ws_create", "radik_ws_destroy", "radik_ws_bytes", "radik_ws_error", "radik_ws_prepare",
-    "radik_topk_radix_select", "radik_topk", "radik_topk_host",
+    "radik_topk_radix_select", "radik_topk", "radik_topk_host", "radik_topk_noalloc",
     "radik_count_bin_ex", "radik_count_bin", "radik_select_bin", "radik_filter",
     "radik_last_error", "radik_status_string", "radik_version",
 )
@@ -58,6 +58,7 @@ def _declare(L: ctypes.CDLL) -> None:
     L.radik_topk_radix_select.argtypes = [P, P, I, P, P, P, P, I64, I64, U32, P]
     L.radik_topk.argtypes = [P, P, I, P, I64, P, I64, P, I64, I64, I, I, P]
     L.radik_topk_host.argtypes = [P, P, I, P, I64, P, I64, P, I64, I64, I, I, P, P]
+    L.radik_topk_noalloc.argtypes = [P, P, I, P, P, P, I64, I64, U32, P]
     L.radik_count_bin_ex.argtypes = [P, P, P, I64, I, I, I, I, P]
     L.radik_count_bin.argtypes = [P, P, P, I64, I64, I, I, P]
     L.radik_select_bin.argtypes = [P, P, P, P, I64, I64, I, P]

@@ -197,19 +197,10 @@ size_t fused_cap(size_t k, size_t tile, int threads) {
     return round_up(cap, 64);
 }
 
-// Build the launch plan for a batch shape (host only).
-int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes) {
-    Plan& pl = ws->plan;
-    PlanKey key;
-    key.lens.assign(lens, lens + T);
-    key.k = k;
-    key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
-    key.idx_bytes = idx_bytes;
-    if (pl.valid && pl.key == key) return RADIK_OK;
-
+// Host half of a launch plan: kernel configuration, segment table, sample
+// jobs and descriptor offsets.  Allocates no device memory.
+int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& np) {
     const DeviceInfo di = device_info();
-    Plan np;
-    np.key = key;
     np.T = T;
     np.N = 0;
     for (int64_t t = 0; t < T; ++t) np.N += lens[t];
@@ -314,14 +305,36 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
                      [](const FusedSeg& a, const FusedSeg& b) { return a.len > b.len; });
     np.nsegs = static_cast<int32_t>(np.segs.size());
     np.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(np.nsegs, resident)));
-    np.valid = true;
-
-    // Device buffers.
-    const StateLayout L(T);
     np.tasks_off = 0;
     np.segs_off = round_up(sizeof(FusedTask) * T, 256);
     np.jobs_off = np.segs_off + round_up(sizeof(FusedSeg) * np.segs.size(), 256);
-    const size_t desc_bytes = np.jobs_off + sizeof(SampleJob) * np.jobs.size();
+    np.valid = true;
+    return RADIK_OK;
+}
+
+// Size of the descriptor block (tasks, segments, sample jobs) of a plan.
+size_t plan_desc_bytes(const Plan& pl) { return pl.jobs_off + sizeof(SampleJob) * pl.jobs.size(); }
+
+// Build the launch plan for a batch shape and size the workspace for it.
+int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes) {
+    Plan& pl = ws->plan;
+    PlanKey key;
+    key.lens.assign(lens, lens + T);
+    key.k = k;
+    key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
+    key.idx_bytes = idx_bytes;
+    if (pl.valid && pl.key == key) return RADIK_OK;
+
+    Plan np;
+    np.key = key;
+    int rc = plan_shape(lens, T, k, flags, np);
+    if (rc) return rc;
+    const bool scale = (flags & RADIK_WITHSCALE) != 0;
+    const size_t kk = static_cast<size_t>(k);
+
+    // Device buffers.
+    const StateLayout L(T);
+    const size_t desc_bytes = plan_desc_bytes(np);
     cudaError_t e = ws->state.ensure(L.bytes);
     if (e == cudaSuccess) e = ws->desc.ensure(desc_bytes);
     if (e == cudaSuccess && np.fused) {
@@ -734,6 +747,153 @@ int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const floa
                                    cudaMemcpyDeviceToHost, s));
     }
     return finish_sync(ws, s);
+}
+
+}  // extern "C"
+
+// ---- allocation-free entry point --------------------------------------------
+//
+// radik_topk_noalloc runs the fused kernel with its scratch (per-call state,
+// plan descriptors, candidate regions of multi-segment tasks, sampled
+// thresholds) in one statically sized device array instead of a workspace.
+// It exists for callers that must not allocate device memory at the point
+// of the call: code running inside a memory pool's out-of-memory handler or
+// an allocator callback, processes with a hard device-memory cap, and
+// latency-critical loops that cannot afford cudaMalloc's implicit device
+// synchronisation.
+
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per device
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+char* g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Per-device set-up: the device address of the static scratch and the
+// shared-memory attribute of the sampling kernels.  Runs once per device, on
+// the first call there.
+int noalloc_setup(int dev, char** base) {
+    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(RADIK_ERR_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_base[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(RADIK_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+        const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
+        for (bool scale : {false, true}) {
+            e = cudaFuncSetAttribute(reinterpret_cast<const void*>(pick_sample(scale)),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ssmem));
+            if (e != cudaSuccess) return fail(RADIK_ERR_CUDA, std::string("sampling kernel: ") + cudaGetErrorString(e));
+        }
+        g_noalloc_base[dev] = static_cast<char*>(p);
+    }
+    *base = g_noalloc_base[dev];
+    return RADIK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_val_in, const void* d_idx_in,
+                       const int64_t* h_task_lens, int64_t num_tasks, int64_t k, uint32_t flags, void* stream) {
+    if (num_tasks < 0 || k < 0) return fail(RADIK_ERR_INVALID, "num_tasks and k must be non-negative");
+    if (idx_bytes != 4 && idx_bytes != 8) return fail(RADIK_ERR_INVALID, "index width must be 4 or 8 bytes");
+    if (flags & (RADIK_PLAIN | RADIK_ASYNC))
+        return fail(RADIK_ERR_INVALID, "radik_topk_noalloc runs the fused path synchronously; "
+                                       "RADIK_PLAIN and RADIK_ASYNC are not accepted");
+    if ((flags & RADIK_WITHIDXIN) && !d_idx_in) return fail(RADIK_ERR_INVALID, "WITHIDXIN needs idx_in");
+    if (k > static_cast<int64_t>(kBitonicMax)) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "radik_topk_noalloc supports k <= %u (got k = %lld)", kBitonicMax,
+                      static_cast<long long>(k));
+        return fail(RADIK_ERR_WS_TOO_SMALL, buf);
+    }
+    if (num_tasks == 0 || k == 0) return RADIK_OK;
+    if (!d_val_out || !d_idx_out || !h_task_lens) return fail(RADIK_ERR_INVALID, "NULL output or task_lens");
+    int64_t maxlen = 0;
+    int rc = validate_lens(h_task_lens, num_tasks, &maxlen);
+    if (rc) return rc;
+    if (maxlen > 0 && !d_val_in) return fail(RADIK_ERR_INVALID, "val_in is NULL");
+    if ((reinterpret_cast<uintptr_t>(d_val_in) & 3) || (reinterpret_cast<uintptr_t>(d_val_out) & 3) ||
+        (reinterpret_cast<uintptr_t>(d_idx_out) & (idx_bytes - 1)) ||
+        ((flags & RADIK_WITHIDXIN) && (reinterpret_cast<uintptr_t>(d_idx_in) & (idx_bytes - 1))))
+        return fail(RADIK_ERR_INVALID, "device arrays must be aligned to their element size");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    RADIK_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone)
+        return fail(RADIK_ERR_CAPTURE, "radik_topk_noalloc uploads its plan and waits for the stream; "
+                                       "it cannot run while the stream captures");
+    int dev = 0;
+    RADIK_CUDA(cudaGetDevice(&dev));
+    char* base = nullptr;
+    rc = noalloc_setup(dev, &base);
+    if (rc) return rc;
+
+    // A workspace view whose buffers all point into the static scratch; it
+    // owns nothing and is never passed to radik_ws_destroy.
+    radik_ws view;
+    view.device = dev;
+    view.n = maxlen;
+    view.num_tasks = num_tasks;
+    view.index_bytes = idx_bytes;
+    rc = plan_shape(h_task_lens, num_tasks, k, flags, view.plan);
+    if (rc) return rc;
+    const Plan& pl = view.plan;
+    if (!pl.fused) return fail(RADIK_ERR_WS_TOO_SMALL, "the fused kernel's candidate buffer does not fit for this k");
+    const StateLayout L(num_tasks);
+    const size_t desc_off = round_up(L.bytes, 256);
+    const size_t cand_off = round_up(desc_off + plan_desc_bytes(pl), 256);
+    const size_t samp_off = round_up(cand_off + sizeof(uint64_t) * static_cast<size_t>(pl.cand_entries), 256);
+    const size_t need = samp_off + sizeof(uint64_t) * static_cast<size_t>(pl.sample_entries);
+    if (need > kNoAllocScratchBytes) {
+        char buf[200];
+        std::snprintf(buf, sizeof(buf),
+                      "radik_topk_noalloc needs %zu bytes of scratch for this batch; its static scratch holds %zu",
+                      need, kNoAllocScratchBytes);
+        return fail(RADIK_ERR_WS_TOO_SMALL, buf);
+    }
+    view.state.p = base;
+    view.state.bytes = L.bytes;
+    view.desc.p = base + desc_off;
+    view.desc.bytes = plan_desc_bytes(pl);
+    view.cand.p = base + cand_off;
+    view.cand.bytes = sizeof(uint64_t) * static_cast<size_t>(pl.cand_entries);
+    view.samples.p = base + samp_off;
+    view.samples.bytes = sizeof(uint64_t) * static_cast<size_t>(pl.sample_entries);
+
+    // Everything that must start at zero (error word, work counters, global
+    // thresholds, done/candidate counters, retry flags) is cleared here; the
+    // descriptors are uploaded from pageable host memory, which the runtime
+    // stages before this call returns.
+    RADIK_CUDA(cudaMemsetAsync(base, 0, L.bytes, s));
+    RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.tasks_off), pl.tasks.data(), sizeof(FusedTask) * pl.T,
+                               cudaMemcpyHostToDevice, s));
+    if (!pl.segs.empty())
+        RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.segs_off), pl.segs.data(), sizeof(FusedSeg) * pl.segs.size(),
+                                   cudaMemcpyHostToDevice, s));
+    if (!pl.jobs.empty())
+        RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.jobs_off), pl.jobs.data(), sizeof(SampleJob) * pl.jobs.size(),
+                                   cudaMemcpyHostToDevice, s));
+    FusedParams p = fused_params(&view, d_val_out, d_idx_out, idx_bytes, d_val_in, d_idx_in, k, flags);
+    rc = run_fused(&view, p, flags, s);
+    if (rc) return rc;
+    uint32_t h_err = 0;
+    RADIK_CUDA(cudaMemcpyAsync(&h_err, err_ptr(&view), sizeof(h_err), cudaMemcpyDeviceToHost, s));
+    RADIK_CUDA(cudaStreamSynchronize(s));
+    if (h_err) {
+        char buf[128];
+        std::snprintf(buf, sizeof(buf), "device error word 0x%x (capacity=1 bounds=2 timeout=4 internal=8)", h_err);
+        return fail((h_err & kErrTimeout) ? RADIK_ERR_TIMEOUT : RADIK_ERR_DEVICE, buf);
+    }
+    return RADIK_OK;
 }
 
 // ---- stage entry points ----------------------------------------------------
