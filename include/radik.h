@@ -70,6 +70,23 @@ int radik_ws_error(radik_ws* ws, uint32_t* bits);
 int radik_ws_prepare(radik_ws* ws, const int64_t* h_task_lens, int64_t num_tasks, int64_t k, uint32_t flags,
                      int idx_bytes);
 
+/* Description of the plan a workspace holds (engine-specific, no reference
+ * counterpart): which kernels a call launches and with what shape. */
+typedef struct radik_plan_info {
+    int path;               /* 0 fused single-read, 1 warp-specialised fused, 2 multi-pass */
+    int block_threads;      /* threads per block of the fused kernel */
+    int grid;               /* blocks of the fused kernel */
+    int smem_bytes;         /* dynamic shared memory per block */
+    int candidate_capacity; /* shared candidate buffer, composites */
+    int segments;           /* work items (task segments) */
+    int sample_jobs;        /* blocks of the sampling kernel (0: not launched) */
+    int kernels_per_call;   /* kernels one call launches (multi-pass: lower bound) */
+} radik_plan_info;
+
+/* Fills *info from the plan built by the last prepare or call; fails with
+ * RADIK_ERR_INVALID when the workspace has no plan yet. */
+int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info);
+
 /* topk_radix_select!(val_out, idx_out, ws, val_in, idx_in, task_lens, k,
  *                    Val(LARGEST), Val(ASCEND), Val(WITHSCALE), Val(WITHIDXIN),
  *                    Val(WITHPACKING), Val(VLOAD_SIZE_BYTES))

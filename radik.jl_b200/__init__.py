@@ -127,6 +127,13 @@ class RadiKWorkspace:
         check(load().radik_ws_prepare(self._h, lens.ctypes.data_as(ctypes.c_void_p), len(lens), int(k),
                                       flags, ib))
 
+    def plan_info(self) -> dict:
+        """The plan the workspace holds (kernel form, grid, launches per call)."""
+        from ._lib import PlanInfo
+        info = PlanInfo()
+        check(load().radik_ws_plan_info(self._h, ctypes.byref(info)))
+        return {n: getattr(info, n) for n, _ in PlanInfo._fields_}
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             load().radik_ws_destroy(self._h)

@@ -29,10 +29,18 @@ STATUS = {
 # Every symbol include/radik.h declares (checked by the CPU test suite).
 EXPORTS = (
     "radik_ws_create", "radik_ws_destroy", "radik_ws_bytes", "radik_ws_error", "radik_ws_prepare",
+    "radik_ws_plan_info",
     "radik_topk_radix_select", "radik_topk", "radik_topk_host", "radik_topk_noalloc",
     "radik_count_bin_ex", "radik_count_bin", "radik_select_bin", "radik_filter",
     "radik_last_error", "radik_status_string", "radik_version",
 )
+
+
+class PlanInfo(ctypes.Structure):
+    """radik_plan_info (include/radik.h)."""
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "path", "block_threads", "grid", "smem_bytes", "candidate_capacity", "segments", "sample_jobs",
+        "kernels_per_call")]
 
 
 class RadiKError(Exception):
@@ -55,6 +63,7 @@ def _declare(L: ctypes.CDLL) -> None:
     L.radik_ws_bytes.argtypes = [P, ctypes.POINTER(ctypes.c_size_t)]
     L.radik_ws_error.argtypes = [P, ctypes.POINTER(U32)]
     L.radik_ws_prepare.argtypes = [P, P, I64, I64, U32, I]
+    L.radik_ws_plan_info.argtypes = [P, ctypes.POINTER(PlanInfo)]
     L.radik_topk_radix_select.argtypes = [P, P, I, P, P, P, P, I64, I64, U32, P]
     L.radik_topk.argtypes = [P, P, I, P, I64, P, I64, P, I64, I64, I, I, P]
     L.radik_topk_host.argtypes = [P, P, I, P, I64, P, I64, P, I64, I64, I, I, P, P]

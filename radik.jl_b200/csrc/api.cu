@@ -12,6 +12,7 @@
 
 #include "../../include/radik.h"
 #include "fused.cuh"
+#include "fused_ws.cuh"
 #include "general.cuh"
 #include "sample.cuh"
 #include "stages.cuh"
@@ -90,10 +91,30 @@ FusedKernel pick_fused(int threads, int vec, bool scale) {
     return nullptr;
 }
 
+// Warp-specialised form: `threads` consumer threads plus one producer warp;
+// a ring of `stages` warp tiles of 128 * j elements (j float4 per lane).
+template <int NCW, int J, int ST, bool S>
+FusedKernel fused_ws_ptr() { return fused_ws_kernel<NCW, J, ST, S>; }
+
+FusedKernel pick_fused_ws(int threads, int j, bool scale) {
+    if (threads == 256 && j == 8) return scale ? fused_ws_ptr<8, 8, 16, true>() : fused_ws_ptr<8, 8, 16, false>();
+    if (threads == 256 && j == 4) return scale ? fused_ws_ptr<8, 4, 24, true>() : fused_ws_ptr<8, 4, 24, false>();
+    return nullptr;
+}
+
+int ws_stages(int j) { return j == 8 ? 16 : 24; }
+
 // Dynamic shared memory of the fused kernel: TMA ring, candidate buffer,
 // one mbarrier per ring stage.
 size_t fused_smem(uint32_t cap, int threads, int vec) {
     return static_cast<size_t>(kStages) * threads * vec * sizeof(float) + static_cast<size_t>(cap) * 8 + kStages * 8;
+}
+
+// Warp-specialised form: ring, candidate buffer, "full" and "empty" mbarrier
+// per stage, the item ring's barriers.
+size_t fused_ws_smem(uint32_t cap, int j) {
+    const size_t st = static_cast<size_t>(ws_stages(j));
+    return st * 128 * j * sizeof(float) + static_cast<size_t>(cap) * 8 + (2 * st + 2 * kItemSlots) * 8;
 }
 
 using SampleKernel = void (*)(FusedParams, const SampleJob*, uint64_t*, uint32_t*);
@@ -126,7 +147,9 @@ struct Plan {
     PlanKey key;
     bool valid = false;
     bool fused = false;
+    bool ws_form = false;   // warp-specialised fused kernel
     int threads = 256, vec = 16;
+    int launch_threads = 256;  // threads plus the producer warp of the warp-specialised form
     uint32_t cap = 0;
     int grid = 0;
     size_t smem = 0;
@@ -210,12 +233,23 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     np.threads = env_int("RADIK_THREADS", 256);
     np.vec = env_int("RADIK_VEC", 8);
     const bool scale = (flags & RADIK_WITHSCALE) != 0;
-    FusedKernel fk = pick_fused(np.threads, np.vec, scale);
-    if (!fk) return fail(RADIK_ERR_INVALID, "unsupported RADIK_THREADS/RADIK_VEC combination");
-    const size_t tile = static_cast<size_t>(np.threads) * np.vec;
     const size_t kk = static_cast<size_t>(k);
-    np.cap = static_cast<uint32_t>(fused_cap(kk, tile, np.threads));
-    np.smem = fused_smem(np.cap, np.threads, np.vec);
+    // Kernel form: the warp-specialised kernel (fused_ws.cuh) unless its
+    // larger ring leaves room for fewer than two blocks per SM, in which case
+    // the single-barrier form (fused.cuh) keeps more bytes in flight.
+    // RADIK_WS=0/1 forces a form.
+    np.cap = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(np.threads) * np.vec, np.threads));
+    const int ws_env = env_int("RADIK_WS", -1);
+    const int ws_j = env_int("RADIK_WSJ", 8);  // float4 per lane in a warp tile
+    np.ws_form = ws_env >= 0 ? ws_env != 0
+                             : (np.threads == 256 && 2 * (fused_ws_smem(np.cap, ws_j) + 2048) <=
+                                                         static_cast<size_t>(di.max_smem_optin));
+    if (np.ws_form) np.vec = ws_j;
+    FusedKernel fk = np.ws_form ? pick_fused_ws(np.threads, np.vec, scale) : pick_fused(np.threads, np.vec, scale);
+    if (!fk) return fail(RADIK_ERR_INVALID, "unsupported RADIK_THREADS/RADIK_VEC combination");
+    np.launch_threads = np.threads + (np.ws_form ? 32 : 0);
+    const size_t tile = static_cast<size_t>(np.threads) * np.vec;
+    np.smem = np.ws_form ? fused_ws_smem(np.cap, np.vec) : fused_smem(np.cap, np.threads, np.vec);
     np.fused = (flags & RADIK_PLAIN) == 0 && np.smem <= static_cast<size_t>(di.max_smem_optin) - 4096;
 
     int occ = 1;
@@ -226,7 +260,8 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
             cudaFuncSetAttribute(reinterpret_cast<const void*>(fk), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(np.smem));
         }
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fk, np.threads, np.smem) != cudaSuccess || occ < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fk, np.launch_threads, np.smem) != cudaSuccess ||
+            occ < 1)
             occ = 1;
     }
     const int64_t resident = static_cast<int64_t>(occ) * di.sms;
@@ -305,6 +340,8 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
                      [](const FusedSeg& a, const FusedSeg& b) { return a.len > b.len; });
     np.nsegs = static_cast<int32_t>(np.segs.size());
     np.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(np.nsegs, resident)));
+    const int grid_cap = env_int("RADIK_GRID", 0);  // fewer CTAs than resident (tests: many items per CTA)
+    if (grid_cap > 0 && np.fused) np.grid = std::min(np.grid, grid_cap);
     np.tasks_off = 0;
     np.segs_off = round_up(sizeof(FusedTask) * T, 256);
     np.jobs_off = np.segs_off + round_up(sizeof(FusedSeg) * np.segs.size(), 256);
@@ -421,8 +458,8 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
             p, ws->desc.as<SampleJob>(pl.jobs_off), ws->samples.as<uint64_t>(), ws->state.as<uint32_t>(L.sdone));
         RADIK_CUDA(cudaGetLastError());
     }
-    FusedKernel fk = pick_fused(pl.threads, pl.vec, scale);
-    fk<<<pl.grid, pl.threads, pl.smem, s>>>(p);
+    FusedKernel fk = pl.ws_form ? pick_fused_ws(pl.threads, pl.vec, scale) : pick_fused(pl.threads, pl.vec, scale);
+    fk<<<pl.grid, pl.launch_threads, pl.smem, s>>>(p);
     RADIK_CUDA(cudaGetLastError());
     if (!pl.jobs.empty()) {
         // Recompute, without the sampled threshold, any task whose seeded
@@ -433,7 +470,7 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
         r.gthr = ws->state.as<uint64_t>(L.gthr_r);
         r.task_done = ws->state.as<uint32_t>(L.done_r);
         r.task_cnt = ws->state.as<uint32_t>(L.cnt_r);
-        fk<<<pl.grid, pl.threads, pl.smem, s>>>(r);
+        fk<<<pl.grid, pl.launch_threads, pl.smem, s>>>(r);
         RADIK_CUDA(cudaGetLastError());
     }
     return RADIK_OK;
@@ -618,6 +655,23 @@ int radik_ws_error(radik_ws* ws, uint32_t* bits) {
     *bits = *ws->h_err;
     RADIK_CUDA(cudaMemsetAsync(err_ptr(ws), 0, 4, ws->last_stream));
     RADIK_CUDA(cudaStreamSynchronize(ws->last_stream));
+    return RADIK_OK;
+}
+
+int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
+    if (!ws || !info) return fail(RADIK_ERR_INVALID, "NULL argument");
+    const Plan& pl = ws->plan;
+    if (!pl.valid) return fail(RADIK_ERR_INVALID, "the workspace has no plan yet");
+    info->path = !pl.fused ? 2 : (pl.ws_form ? 1 : 0);
+    info->block_threads = pl.fused ? pl.launch_threads : 256;
+    info->grid = pl.grid;
+    info->smem_bytes = static_cast<int>(pl.smem);
+    info->candidate_capacity = static_cast<int>(pl.cap);
+    info->segments = pl.nsegs;
+    info->sample_jobs = static_cast<int>(pl.jobs.size());
+    // fused: sampling kernel + fused kernel + retry launch when sampled;
+    // multi-pass: histogram, select, compact, advance, finalize at least.
+    info->kernels_per_call = pl.fused ? (pl.jobs.empty() ? 1 : 3) : 5;
     return RADIK_OK;
 }
 

@@ -50,11 +50,11 @@ __device__ __forceinline__ void block_or_and(uint64_t& vor, uint64_t& vand, Bloc
     }
     const int w = threadIdx.x >> 5;
     if (lane_id() == 0) { s.warp_a[w] = vor; s.warp_b[w] = vand; }
-    __syncthreads();
+    block_sync<THREADS>();
     vor = 0; vand = ~0ull;
 #pragma unroll
     for (int i = 0; i < BlockScratch<THREADS>::kWarps; ++i) { vor |= s.warp_a[i]; vand &= s.warp_b[i]; }
-    __syncthreads();
+    block_sync<THREADS>();
 }
 
 template <int THREADS>
@@ -63,11 +63,11 @@ __device__ __forceinline__ uint64_t block_min_u64(uint64_t v, BlockScratch<THREA
     for (int m = 16; m > 0; m >>= 1) { uint64_t o = shfl_xor_u64(v, m); v = o < v ? o : v; }
     const int w = threadIdx.x >> 5;
     if (lane_id() == 0) s.warp_a[w] = v;
-    __syncthreads();
+    block_sync<THREADS>();
     v = ~0ull;
 #pragma unroll
     for (int i = 0; i < BlockScratch<THREADS>::kWarps; ++i) v = s.warp_a[i] < v ? s.warp_a[i] : v;
-    __syncthreads();
+    block_sync<THREADS>();
     return v;
 }
 
@@ -77,11 +77,11 @@ __device__ __forceinline__ uint32_t block_sum_u32(uint32_t v, BlockScratch<THREA
     for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(kFullMask, v, m);
     const int w = threadIdx.x >> 5;
     if (lane_id() == 0) s.warp_u32[w] = v;
-    __syncthreads();
+    block_sync<THREADS>();
     v = 0;
 #pragma unroll
     for (int i = 0; i < BlockScratch<THREADS>::kWarps; ++i) v += s.warp_u32[i];
-    __syncthreads();
+    block_sync<THREADS>();
     return v;
 }
 
@@ -91,7 +91,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
     uint32_t inc = warp_inclusive_scan<true>(v);
     const int w = threadIdx.x >> 5;
     if (lane_id() == 31) s.warp_u32[w] = inc;
-    __syncthreads();
+    block_sync<THREADS>();
     uint32_t before = 0, all = 0;
 #pragma unroll
     for (int i = 0; i < BlockScratch<THREADS>::kWarps; ++i) {
@@ -99,7 +99,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* t
         before += (i < w) ? x : 0u;
         all += x;
     }
-    __syncthreads();
+    block_sync<THREADS>();
     *total = all;
     return before + inc - v;
 }
@@ -145,7 +145,7 @@ __device__ __forceinline__ void block_rank_search(uint32_t r, uint32_t nb, Block
             }
         }
     }
-    __syncthreads();
+    block_sync<THREADS>();
 }
 
 // Ordered in-place compaction: moves the entries of buf[0, cnt) that are
@@ -181,7 +181,7 @@ __device__ __forceinline__ uint32_t block_compact_ge(uint64_t* buf, uint32_t cnt
             }
         }
         out += total;
-        __syncthreads();
+        block_sync<THREADS>();
     }
     *mn_out = block_min_u64<THREADS>(mn, s);
     return out;
@@ -222,7 +222,7 @@ __device__ uint32_t block_shrink(uint64_t* buf, uint32_t cnt, uint32_t k, uint32
         const int sh = top + 1 - w;
         const uint32_t nb = 1u << w;
         for (uint32_t i = tid; i < nb; i += THREADS) s.hist[i] = 0;
-        __syncthreads();
+        block_sync<THREADS>();
         const uint64_t dmask = nb - 1;
         for (uint32_t base = 0; base < n; base += THREADS) {
             const uint32_t i = base + tid;
@@ -230,10 +230,10 @@ __device__ uint32_t block_shrink(uint64_t* buf, uint32_t cnt, uint32_t k, uint32
             const bool in = i < n && (pbits == 0 || (c >> (sh + w)) == prefix);
             warp_hist_add(s.hist, static_cast<uint32_t>((c >> sh) & dmask), in);
         }
-        __syncthreads();
+        block_sync<THREADS>();
         block_rank_search<THREADS>(r, nb, s);
         const uint32_t b = s.bc32[0], rr = s.bc32[1], cb = s.bc32[2], ab = s.bc32[3];
-        __syncthreads();
+        block_sync<THREADS>();
         if (cb == 0xffffffffu) {  // rank beyond the entries: inputs outside [lo, hi]
             if (tid == 0) record_error(err, kErrInternal);
             keep_from = lo;
@@ -276,7 +276,7 @@ __device__ uint64_t block_rank_threshold(const uint64_t* buf, uint32_t n, uint32
         const int sh = top + 1 - w;
         const uint32_t nb = 1u << w;
         for (uint32_t i = tid; i < nb; i += THREADS) s.hist[i] = 0;
-        __syncthreads();
+        block_sync<THREADS>();
         const uint64_t dmask = nb - 1;
         for (uint32_t base = 0; base < n; base += THREADS) {
             const uint32_t i = base + tid;
@@ -284,10 +284,10 @@ __device__ uint64_t block_rank_threshold(const uint64_t* buf, uint32_t n, uint32
             const bool in = i < n && (pbits == 0 || (c >> (sh + w)) == prefix);
             warp_hist_add(s.hist, static_cast<uint32_t>((c >> sh) & dmask), in);
         }
-        __syncthreads();
+        block_sync<THREADS>();
         block_rank_search<THREADS>(r, nb, s);
         const uint32_t b = s.bc32[0], rr = s.bc32[1], cb = s.bc32[2], ab = s.bc32[3];
-        __syncthreads();
+        block_sync<THREADS>();
         if (cb == 0xffffffffu) return keep_from;
         prefix = (pbits == 0) ? b : ((prefix << w) | b);
         pbits += w;
@@ -328,7 +328,7 @@ __device__ __forceinline__ void bitonic_sort_u64(uint64_t* a, uint32_t n, bool d
                 uint64_t x = a[lo], y = a[hi];
                 if ((x > y) == asc) { a[lo] = y; a[hi] = x; }
             }
-            __syncthreads();
+            block_sync<THREADS>();
         }
     }
 }
@@ -351,12 +351,12 @@ __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, ui
         if (((diff >> sh) & 0xffull) == 0) continue;
         // digit histogram -> exclusive offsets
         for (int i = tid; i < 256; i += THREADS) s.hist[i] = 0;
-        __syncthreads();
+        block_sync<THREADS>();
         for (uint32_t base = 0; base < n; base += THREADS) {
             const uint32_t i = base + tid;
             warp_hist_add(s.hist, i < n ? static_cast<uint32_t>((a[i] >> sh) & 0xff) : 0u, i < n);
         }
-        __syncthreads();
+        block_sync<THREADS>();
         if (tid < 32) {
             uint32_t c[8], sum = 0;
 #pragma unroll
@@ -366,7 +366,7 @@ __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, ui
 #pragma unroll
             for (int j = 0; j < 8; ++j) { digit_base[tid * 8 + j] = run; run += c[j]; }
         }
-        __syncthreads();
+        block_sync<THREADS>();
         // stable scatter, one tile of THREADS keys at a time in order
         for (uint32_t base = 0; base < n; base += THREADS) {
             uint32_t i = base + tid;
@@ -376,9 +376,9 @@ __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, ui
             uint32_t peers = __match_any_sync(kFullMask, d);
             uint32_t rank = __popc(peers & lanemask_lt());
             for (int j = tid; j < W * 256; j += THREADS) warp_digit[j] = 0;
-            __syncthreads();
+            block_sync<THREADS>();
             if (valid && rank == 0) warp_digit[w * 256 + d] = __popc(peers);
-            __syncthreads();
+            block_sync<THREADS>();
             // per digit: prefix over warps (thread d handles digit d)
             for (int dd = tid; dd < 256; dd += THREADS) {
                 uint32_t run = digit_base[dd];
@@ -389,9 +389,9 @@ __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, ui
                 }
                 digit_base[dd] = run;
             }
-            __syncthreads();
+            block_sync<THREADS>();
             if (valid) b[warp_digit[w * 256 + d] + rank] = v;
-            __syncthreads();
+            block_sync<THREADS>();
         }
         uint64_t* t = a; a = b; b = t;
     }

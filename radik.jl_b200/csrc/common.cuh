@@ -140,6 +140,31 @@ __device__ __forceinline__ T warp_inclusive_scan(T v) {
     return v;
 }
 
+// Barrier over the first THREADS threads of the CTA (hardware barrier 1).
+// In a kernel whose block has exactly THREADS threads it is __syncthreads();
+// the fused kernel's consumer warps use it without the producer warp that
+// feeds them.  Same rules as __syncthreads: every participating warp reaches
+// it, without divergence.
+template <int THREADS>
+__device__ __forceinline__ void block_sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(THREADS) : "memory");
+}
+
+// block_sync that also returns whether `pred` holds in any participating thread.
+template <int THREADS>
+__device__ __forceinline__ bool block_sync_or(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(static_cast<uint32_t>(pred)), "n"(THREADS)
+        : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ void record_error(uint32_t* err, uint32_t bits) {
     if (err) atomicOr(err, bits);
 }

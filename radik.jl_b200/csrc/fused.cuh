@@ -202,7 +202,7 @@ __device__ void write_row(const FusedParams& p, const TaskView& tv, const uint64
         if (p.idx_bytes == 8) static_cast<int64_t*>(tv.iout)[j] = idx;
         else static_cast<int32_t*>(tv.iout)[j] = static_cast<int32_t>(idx);
     }
-    __syncthreads();
+    block_sync<THREADS>();
 }
 
 // Sort the m finished composites of a task by the output order, map indices
@@ -230,13 +230,13 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
             buf[i] = output_sort_key(bits, pos, tv.sp, tv.ascend);
         }
     }
-    __syncthreads();
+    block_sync<THREADS>();
     uint64_t* sorted = buf;
     if (m <= kBitonicMax) {
         uint32_t P = 1;
         while (P < m) P <<= 1;
         for (uint32_t i = m + tid; i < P; i += THREADS) buf[i] = ~0ull;
-        __syncthreads();
+        block_sync<THREADS>();
         bitonic_sort_u64<THREADS>(buf, P);
     } else {
         uint64_t* scratch = p.sort_scratch + static_cast<int64_t>(blockIdx.x) * p.kmax;
@@ -244,7 +244,7 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
         uint32_t* db = wd + (THREADS / 32) * 256;
         sorted = radix_sort_u64<THREADS>(buf, scratch, m, sh.bs, wd, db);
     }
-    __syncthreads();
+    block_sync<THREADS>();
     write_row<THREADS, kFromScore>(p, tv, sorted, m);
 }
 
@@ -255,9 +255,9 @@ __device__ __forceinline__ uint32_t buffer_count(const FusedParams& p, FusedShar
     uint32_t cnt = sh.cnt;
     if (cnt > p.cap) {
         cnt = p.cap;
-        __syncthreads();
+        block_sync<THREADS>();
         if (threadIdx.x == 0) sh.cnt = cnt;
-        __syncthreads();
+        block_sync<THREADS>();
     }
     return cnt;
 }
@@ -273,9 +273,9 @@ __device__ uint64_t shrink_mid(const FusedParams& p, uint32_t k, uint32_t max_ke
     block_or_and<THREADS>(vor, vand, sh.bs);
     uint64_t kf = 0, mn = 0;
     const uint32_t kept = block_shrink<THREADS>(buf, cnt, k, max_keep, vand, vor, sh.bs, p.err, &kf, &mn);
-    __syncthreads();
+    block_sync<THREADS>();
     if (threadIdx.x == 0) sh.cnt = kept;
-    __syncthreads();
+    block_sync<THREADS>();
     return (kept >= k && kept < cnt) ? kf : 0ull;
 }
 
@@ -287,9 +287,9 @@ __device__ uint32_t shrink_final(const FusedParams& p, uint32_t k, uint64_t* buf
     const uint32_t cnt = buffer_count<THREADS>(p, sh);
     uint32_t m = block_select_topk<THREADS>(buf, cnt, k, sh.bs, p.err, kth);
     if (m < k) *kth = 0;
-    __syncthreads();
+    block_sync<THREADS>();
     if (threadIdx.x == 0) sh.cnt = m;
-    __syncthreads();
+    block_sync<THREADS>();
     return m;
 }
 
@@ -318,7 +318,7 @@ __device__ uint64_t sampled_threshold(const TaskView& tv, float scaler, uint32_t
     }
     block_or_and<THREADS>(vor, vand, sh.bs);  // barriers: the sample is in buf
     const uint64_t kf = block_rank_threshold<THREADS>(buf, S, r, 4 * r, vand, vor, sh.bs);
-    __syncthreads();
+    block_sync<THREADS>();
     return kf > 0 ? kf - 1 : 0ull;
 }
 
@@ -334,7 +334,7 @@ __device__ void gather_regions(uint64_t* s_buf, uint32_t cap_s, uint32_t& wcnt, 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t wc = wcnt < R ? wcnt : R;
     if (lane == 0) sh.wc[warp] = wc;
-    __syncthreads();
+    block_sync<THREADS>();
     uint32_t off = sh.cnt, total = sh.cnt;
 #pragma unroll
     for (int i = 0; i < NW; ++i) {
@@ -355,10 +355,10 @@ __device__ void gather_regions(uint64_t* s_buf, uint32_t cap_s, uint32_t& wcnt, 
                 __syncwarp();
             }
         }
-        __syncthreads();
+        block_sync<THREADS>();
     }
     if (threadIdx.x == 0) sh.cnt = total;
-    __syncthreads();
+    block_sync<THREADS>();
     wcnt = 0;
 }
 
@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
         sh.abort = 0;
         sh.work = static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
     }
-    __syncthreads();
+    block_sync<THREADS>();
     uint32_t gtile = 0;      // tiles this CTA consumed so far: ring stage and mbarrier phase
     int w = sh.work;
     bool prefetched = false;  // the current item's first tiles are already in flight
@@ -495,9 +495,9 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
         const int t = G.sg.task;
         int nw = p.nsegs;  // next work item, fetched once this one's tiles are consumed
         if (G.skip) {      // retry launch: only flagged tasks run
-            __syncthreads();
+            block_sync<THREADS>();
             if (tid == 0) sh.work = static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
-            __syncthreads();
+            block_sync<THREADS>();
             w = sh.work;
             prefetched = false;
             continue;
@@ -516,16 +516,16 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
             bool sampled_local = false;
             if (multi) {
                 if (tid == 0) sh.gthr = load_volatile_u64(p.gthr + t);
-                __syncthreads();
+                block_sync<THREADS>();
                 thr = sh.gthr;
             } else if (attempt == 0) {
                 // Overlaps with the tile copies already in flight.
                 thr = sampled_threshold<THREADS, kScale>(tv, scaler, k, s_buf, sh, p.err);
                 sampled_local = thr != 0;
             }
-            __syncthreads();
+            block_sync<THREADS>();
             if (tid == 0) { sh.cnt = 0; sh.gthr = thr; }
-            __syncthreads();
+            block_sync<THREADS>();
             uint32_t wcnt = 0;  // entries in this warp's region (same in all its lanes)
 
             // Head [s0, a0) and tail [a1, s1): fewer than 4 elements each (warp 0).
@@ -641,7 +641,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                 // One barrier per tile; it also tells every thread whether a
                 // warp region runs short, candidates wait for room, or a wait
                 // timed out.
-                if (__syncthreads_or(flag ? 1 : 0)) {
+                if (block_sync_or<THREADS>(flag ? 1 : 0)) {
                     if (sh.abort) {
                         // Drain the copies this CTA still has in flight (bounded).
                         if (tid == 0) {
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                                 mbar_wait_bounded(bars + (gtile + i) % STAGES, ((gtile + i) / STAGES) & 1u,
                                                   kWaitPolls);
                         }
-                        __syncthreads();
+                        block_sync<THREADS>();
                         return;
                     }
                     // Gather the regions, shrink, raise the threshold, and
@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                             }
                             again = dm != 0 || wcnt + RSLACK > R;
                         }
-                        if (!__syncthreads_or(again ? 1 : 0)) break;
+                        if (!block_sync_or<THREADS>(again ? 1 : 0)) break;
                     }
                     if (dm != 0) record_error(p.err, kErrCapacity);
                 }
@@ -721,7 +721,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
         // This item's tiles are all consumed: fetch the next item and start its
         // first tile copies, so they overlap the selection work below.
         if (tid == 0) sh.work = static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
-        __syncthreads();
+        block_sync<THREADS>();
         nw = sh.work;
         if (nw < p.nsegs) {
             TaskView ntv;
@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                 if (kth != 0) atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), kth - 1);
                 sh.gthr = load_volatile_u64(p.gthr + t);
             }
-            __syncthreads();
+            block_sync<THREADS>();
             {
                 const uint64_t g = sh.gthr;
                 const uint32_t cnt = sh.cnt;
@@ -760,22 +760,22 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                     uint32_t total;
                     uint32_t off = block_exclusive_scan<THREADS>(keep ? 1u : 0u, &total, sh.bs);
                     if (tid == 0 && total) sh.base = atomicAdd(p.task_cnt + t, total);
-                    __syncthreads();
+                    block_sync<THREADS>();
                     if (keep) {
                         uint32_t o = sh.base + off;
                         if (o < region) dst[o] = c;
                         else record_error(p.err, kErrCapacity);
                     }
-                    __syncthreads();
+                    block_sync<THREADS>();
                 }
             }
             __threadfence();
-            __syncthreads();
+            block_sync<THREADS>();
             if (tid == 0) {
                 uint32_t done = atomicAdd(p.task_done + t, 1u);
                 sh.last = (done == static_cast<uint32_t>(td.nseg - 1)) ? 1u : 0u;
             }
-            __syncthreads();
+            block_sync<THREADS>();
             if (sh.last) {
                 // Last segment of the task: merge all segments' survivors.
                 __threadfence();
@@ -784,7 +784,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                     sh.gthr = load_volatile_u64(p.gthr + t);
                     sh.base = __ldcg(p.task_cnt + t);
                 }
-                __syncthreads();
+                block_sync<THREADS>();
                 const uint64_t g = sh.gthr;
                 const uint32_t region = static_cast<uint32_t>(td.nseg) * p.kmax;
                 const uint32_t n = sh.base < region ? sh.base : region;
@@ -795,12 +795,12 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                         uint64_t c = (i < n) ? __ldcg(src + i) : 0ull;
                         warp_append((i < n) && c > g, c, s_buf, &sh.cnt, cap, p.err);
                     }
-                    __syncthreads();
+                    block_sync<THREADS>();
                     const uint32_t cnt_now = sh.cnt;
-                    __syncthreads();
+                    block_sync<THREADS>();
                     if (cnt_now > compact_at) shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh);
                 }
-                __syncthreads();
+                block_sync<THREADS>();
                 const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh, &kth);
                 if (m < k && (td.flags & kTaskSampled) && !p.retry) {
                     // The sampled threshold was above the task's k-th composite.
@@ -811,7 +811,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                 }
             }
         }
-        __syncthreads();
+        block_sync<THREADS>();
         w = nw;
         prefetched = next_prefetched;
     }

@@ -1,0 +1,629 @@
+// fused_ws.cuh -- warp-specialised form of the fused top-k kernel.
+//
+// Same work items, thresholds, candidate buffer, retry and finishing as
+// fused_topk_kernel (fused.cuh); what differs is how tiles move and how warps
+// coordinate:
+//   * one producer warp pulls work items from the queue, hands them to the
+//     consumer warps through a small ring of item slots, and streams every
+//     item's tiles with 1-D bulk copies into a ring of shared-memory stages
+//     ("full" mbarrier per stage, completed by the copy's byte count);
+//   * every tile belongs to one consumer warp (tiles are dealt round-robin),
+//     32 elements per lane, so the per-tile cost (wait, release, bookkeeping)
+//     is paid once per 32 elements; the warp frees the stage ("empty"
+//     mbarrier) as soon as it is done with it, and no barrier is shared
+//     between warps while they stream;
+//   * the fast test keeps one bit per lane and float4; only lanes with a
+//     passing group compute element bits, one warp scan places the warp's
+//     candidates in its own region, and the values are read back from the
+//     stage the warp still holds;
+//   * when a warp's region overflows it keeps the tile, raises a request and
+//     every consumer warp joins a block-wide shrink (polling the request
+//     between tiles and while waiting for one), after which the requester
+//     places the rest of its tile with the raised threshold;
+//   * a single-segment task's first two tiles are a sample of it (chunks
+//     spread over the whole task), streamed like any tile so that its
+//     latency overlaps the previous task; its group maxima give the starting
+//     threshold (see ws_sample_rank).
+// Consumer warps synchronise with hardware barrier 1 over THREADS consumer
+// threads (block_sync), so the producer never takes part in their barriers.
+// Every mbarrier wait is bounded; a wait that gives up records a timeout and
+// sets the CTA's abort flag, after which all waits give up at once, the
+// producer stops issuing and waits (bounded) for its copies in flight.
+#pragma once
+
+#include "fused.cuh"
+
+namespace radik {
+
+constexpr int kItemSlots = 4;
+
+template <int THREADS>
+struct WsShared {
+    FusedShared<THREADS> f;
+    uint64_t thr;               // threshold published by the last block-wide shrink
+    int32_t items[kItemSlots];  // work items, producer -> consumers
+    int32_t cur;                // the consumers' current item (written by thread 0)
+    uint32_t req;               // a consumer warp needs room
+    uint32_t arrived;           // consumer warps done with the current item's tiles
+};
+
+__device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t* a) {
+    return *reinterpret_cast<const volatile uint32_t*>(a);
+}
+__device__ __forceinline__ void st_volatile_u32(uint32_t* a, uint32_t v) {
+    *reinterpret_cast<volatile uint32_t*>(a) = v;
+}
+
+// Bounded wait of one thread on one mbarrier phase; gives up early once the
+// CTA aborts.  Returns false when it gave up (a timeout is recorded and the
+// abort flag set).
+__device__ __forceinline__ bool ws_wait(uint64_t* bar, uint32_t parity, uint32_t* abort, uint32_t* err) {
+    for (uint32_t i = 0; i < kWaitPolls; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 63u) == 63u && ld_volatile_u32(abort)) return false;
+    }
+    record_error(err, kErrTimeout);
+    st_volatile_u32(abort, 1u);
+    return false;
+}
+
+// Bounded wait of a whole warp on one mbarrier phase.
+__device__ __forceinline__ bool ws_warp_wait(uint64_t* bar, uint32_t parity, uint32_t* abort, uint32_t* err) {
+    for (uint32_t polls = 1;; ++polls) {
+        if (__all_sync(kFullMask, mbar_try_wait(bar, parity))) return true;
+        if (__any_sync(kFullMask, polls >= kWaitPolls || ((polls & 63u) == 0u && ld_volatile_u32(abort) != 0u))) {
+            if (lane_id() == 0) {
+                record_error(err, kErrTimeout);
+                st_volatile_u32(abort, 1u);
+            }
+            return false;
+        }
+    }
+}
+
+// Sample of a single-segment task: kSampleChunks chunks of kSampleChunkLen
+// consecutive elements spread evenly over the task (kSampleLen elements, the
+// first tiles of the task in the ring).  The consumers take the maximum score
+// of every 4 consecutive sampled elements (a group) and start from the lower
+// edge of the digit bin holding the r-th largest group maximum: at least r
+// groups, hence at least r sampled elements, score at or above it.  With
+// lam = k * kSampleLen / len sampled elements expected at or above the task's
+// k-th score, r = lam + 2 sqrt(lam) + 3 leaves a small chance (about 0.5% at
+// lam = 8) that the threshold is too high; the task is then recomputed
+// without it, so results never depend on the sample.  Returns r, or 0 when
+// the task gets no sample.
+constexpr uint32_t kSampleChunks = 32;
+constexpr uint32_t kSampleChunkLen = 64;
+constexpr uint32_t kSampleLen = kSampleChunks * kSampleChunkLen;
+
+__device__ __forceinline__ uint32_t ws_sample_rank(const FusedTask& td, bool retry) {
+    if (retry || td.nseg != 1 || td.len < 8 * static_cast<int64_t>(kSampleLen)) return 0u;
+    const float lam = static_cast<float>(td.k) * static_cast<float>(kSampleLen) / static_cast<float>(td.len);
+    const uint32_t r = static_cast<uint32_t>(ceilf(lam + 2.0f * sqrtf(lam) + 3.0f));
+    return r <= kSampleLen / 4 / 4 ? r : 0u;  // at most a quarter of the groups
+}
+
+// First element of sample chunk c, 16-byte aligned in memory (mis: the task
+// pointer's offset in elements from a 16-byte boundary).
+__device__ __forceinline__ int64_t ws_sample_pos(int64_t len, int64_t mis, uint32_t c) {
+    int64_t q = ((static_cast<int64_t>(c) * len / kSampleChunks + mis) & ~int64_t(3)) - mis;
+    if (q < 0) q += 4;
+    const int64_t last = ((len - kSampleChunkLen + mis) & ~int64_t(3)) - mis;  // last aligned start that fits
+    return q < last ? q : last;
+}
+
+// Producer (one thread): items to the item ring, tiles to the stage ring.
+template <int THREADS, int J, int STAGES, bool kScale>
+__device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, uint64_t* empty, uint64_t* item_full,
+                            uint64_t* item_empty, WsShared<THREADS>& sh) {
+    constexpr uint32_t TW = 128u * J;  // elements per warp tile
+    constexpr uint32_t kSampleTiles = kSampleLen / TW;
+    constexpr uint32_t kChunksPerTile = TW / kSampleChunkLen;
+    static_assert(kSampleLen % TW == 0 && TW % kSampleChunkLen == 0, "sample tiles");
+    uint32_t g = 0;            // tiles issued
+    uint32_t st = 0, eph = 1;  // stage of tile g; parity of the "empty" phase it must wait for
+    for (uint32_t d = 0;; ++d) {
+        const uint32_t slot = d % kItemSlots;
+        if (d >= kItemSlots && !ws_wait(item_empty + slot, ((d / kItemSlots) - 1u) & 1u, &sh.f.abort, p.err)) break;
+        const int32_t w =
+            ld_volatile_u32(&sh.f.abort) ? p.nsegs : static_cast<int32_t>(atomicAdd(p.work_counter, 1u));
+        sh.items[slot] = w;
+        mbar_arrive(item_full + slot);  // release: the consumers read items[slot] after their wait
+        if (w >= p.nsegs) break;
+        TaskView tv;
+        const SegGeom G = seg_geom<TW, kScale>(p, w, &tv);
+        if (G.skip) continue;
+        bool ok = true;
+        const uint32_t ns = ws_sample_rank(G.td, p.retry != 0) != 0 ? kSampleTiles : 0u;
+        const uint32_t nt = G.ntiles + ns;
+        const int64_t mis = static_cast<int64_t>((reinterpret_cast<uintptr_t>(tv.data) >> 2) & 3);
+        for (uint32_t i = 0; i < nt; ++i, ++g) {
+            if (g >= static_cast<uint32_t>(STAGES) && !ws_wait(empty + st, eph, &sh.f.abort, p.err)) {
+                ok = false;
+                break;
+            }
+            float* dst = ring + static_cast<size_t>(st) * TW;
+            if (i < ns) {
+                mbar_arrive_expect_tx(full + st, TW * 4u);
+                for (uint32_t c = 0; c < kChunksPerTile; ++c)
+                    bulk_load(dst + c * kSampleChunkLen, tv.data + ws_sample_pos(tv.len, mis, i * kChunksPerTile + c),
+                              kSampleChunkLen * 4u, full + st);
+            } else {
+                const int64_t e0 = static_cast<int64_t>(i - ns) * TW;
+                const uint32_t bytes = static_cast<uint32_t>(min(static_cast<int64_t>(TW), G.nvec * 4 - e0)) * 4u;
+                mbar_arrive_expect_tx(full + st, bytes);
+                bulk_load(dst, tv.data + G.a0 + e0, bytes, full + st);
+            }
+            if (++st == static_cast<uint32_t>(STAGES)) { st = 0; eph ^= 1u; }
+        }
+        if (!ok) break;
+    }
+    // Copies still in flight must land before the CTA exits.
+    for (uint32_t j = g > static_cast<uint32_t>(STAGES) ? g - STAGES : 0u; j < g; ++j)
+        mbar_wait_bounded(full + j % STAGES, (j / STAGES) & 1u, kWaitPolls);
+}
+
+// Fast test of a warp tile: bit j of the result is set when some element of
+// this lane's float4 j passes the fast filter.  Float4 j of the lane is
+// src[j * 32 + lane]; only the first nv float4 of the tile are elements.
+template <int J, bool kScale>
+__device__ __forceinline__ uint32_t ws_group_mask(const float4* src, uint32_t nv, uint32_t lane, const FastFilter& ff,
+                                                  float scaler) {
+    float4 x[J];
+    if (nv >= 32u * J) {
+#pragma unroll
+        for (int j = 0; j < J; ++j) x[j] = src[j * 32 + lane];
+    } else {
+#pragma unroll
+        for (int j = 0; j < J; ++j) x[j] = (j * 32 + lane < nv) ? src[j * 32 + lane] : ff.pad4;
+    }
+    if constexpr (kScale) {
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            x[j].x = __fsub_rn(x[j].x, scaler); x[j].y = __fsub_rn(x[j].y, scaler);
+            x[j].z = __fsub_rn(x[j].z, scaler); x[j].w = __fsub_rn(x[j].w, scaler);
+        }
+    }
+    uint32_t gm = 0;
+    if (ff.dir == 0u && !ff.nan_pass) {
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+            gm |= static_cast<uint32_t>((x[j].x >= ff.t) | (x[j].y >= ff.t) | (x[j].z >= ff.t) | (x[j].w >= ff.t)) << j;
+    } else if (!ff.nan_pass) {
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+            gm |= static_cast<uint32_t>((x[j].x <= ff.tr) | (x[j].y <= ff.tr) | (x[j].z <= ff.tr) | (x[j].w <= ff.tr))
+                  << j;
+    } else if (ff.dir == 0u) {
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+            gm |= static_cast<uint32_t>(!(x[j].x < ff.t) | !(x[j].y < ff.t) | !(x[j].z < ff.t) | !(x[j].w < ff.t)) << j;
+    } else {
+#pragma unroll
+        for (int j = 0; j < J; ++j)
+            gm |= static_cast<uint32_t>(!(x[j].x > ff.tr) | !(x[j].y > ff.tr) | !(x[j].z > ff.tr) | !(x[j].w > ff.tr))
+                  << j;
+    }
+    return gm;
+}
+
+// Places candidates of a warp tile in the warp's region.  Element bit
+// b = 4 j + e of a lane is component e of its float4 j (src[j * 32 + lane]).
+// `groups` selects float4 whose elements are tested with the fast filter
+// (initial placement); with groups == 0, `elems` lists elements offered again
+// after a shrink, kept only if their composite beats thr.  One warp scan
+// gives every lane its slots; returns the element bits that found no room.
+template <int J, bool kScale>
+__device__ __forceinline__ uint32_t ws_place(const float4* src, uint32_t groups, uint32_t elems, uint32_t nv,
+                                             uint32_t qb, uint32_t pos0, uint64_t thr, const FastFilter& ff,
+                                             float scaler, const ScoreParams& sp, uint64_t* region, uint32_t R,
+                                             uint32_t& wcnt, uint32_t lane) {
+    const float* srcf = reinterpret_cast<const float*>(src);
+    uint32_t pm = elems;
+    for (uint32_t gs = groups; gs; gs &= gs - 1) {
+        const int j = __ffs(gs) - 1;
+        if (j * 32 + lane >= nv) continue;  // past the end of the segment
+        const float4 f = src[j * 32 + lane];
+        const float fv[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float x = fv[e];
+            if constexpr (kScale) x = __fsub_rn(x, scaler);
+            const float xs = __uint_as_float(__float_as_uint(x) ^ ff.dir);
+            const bool ps = ff.nan_pass ? !(xs < ff.t) : (xs >= ff.t);
+            pm |= static_cast<uint32_t>(ps) << (j * 4 + e);
+        }
+    }
+    if (groups == 0u) {  // offered again: exact test against the raised threshold
+        uint32_t keep = 0;
+        for (uint32_t m = pm; m; m &= m - 1) {
+            const int b = __ffs(m) - 1;
+            const uint32_t q = static_cast<uint32_t>(b >> 2) * 32u + lane;
+            const uint64_t c = make_composite(score_of<kScale>(__float_as_uint(srcf[q * 4 + (b & 3)]), scaler, sp),
+                                              pos0 + (qb + q) * 4u + (b & 3));
+            if (c > thr) keep |= 1u << b;
+        }
+        pm = keep;
+    }
+    const uint32_t n = __popc(pm);
+    const uint32_t incl = warp_inclusive_scan<true>(n);
+    uint32_t slot = wcnt + incl - n;
+    wcnt += __shfl_sync(kFullMask, incl, 31);
+    uint32_t om = 0;
+    for (uint32_t m = pm; m; m &= m - 1) {
+        const int b = __ffs(m) - 1;
+        const uint32_t q = static_cast<uint32_t>(b >> 2) * 32u + lane;
+        const uint64_t c = make_composite(score_of<kScale>(__float_as_uint(srcf[q * 4 + (b & 3)]), scaler, sp),
+                                          pos0 + (qb + q) * 4u + (b & 3));
+        if (slot < R) region[slot] = c;
+        else om |= 1u << b;
+        ++slot;
+    }
+    return om;
+}
+
+template <int NCW, int J, int STAGES, bool kScale>
+__global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams p) {
+    constexpr int THREADS = NCW * 32;             // consumer threads
+    constexpr uint32_t TW = 128u * J;             // elements per warp tile (one ring stage)
+    constexpr uint32_t TW4 = TW / 4;              // float4 per warp tile
+    constexpr uint32_t kSampleTiles = kSampleLen / TW;
+    constexpr uint32_t R = kRegionEntries / NCW;  // append region of each consumer warp
+    static_assert(J * 4 <= 32, "element bits of a lane fit in 32 bits");
+    // Ring tile g sits in stage g % STAGES and belongs to warp g % NCW.  With
+    // STAGES a multiple of NCW every stage belongs to one warp, so the tile a
+    // warp waits for always follows, in its stage, a tile that warp has
+    // already consumed: the stage's barrier is then never more than one phase
+    // behind the awaited one, which a parity wait requires.  (With shared
+    // stages a warp could wait on phase n while phase n - 1, another warp's
+    // tile, was still in flight, and the parity test would pass at once.)
+    static_assert(STAGES % NCW == 0, "every ring stage belongs to one consumer warp");
+    static_assert(kSampleTiles <= static_cast<uint32_t>(NCW), "every sample tile has its own warp");
+    static_assert(kSampleLen / 4 <= kRegionEntries, "group maxima fit in the candidate buffer");
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ WsShared<THREADS> sh;
+    float* ring = reinterpret_cast<float*>(smem_raw);
+    uint64_t* s_buf = reinterpret_cast<uint64_t*>(smem_raw + static_cast<size_t>(STAGES) * TW * 4);
+    uint64_t* full = s_buf + p.cap;
+    uint64_t* empty = full + STAGES;
+    uint64_t* item_full = empty + STAGES;
+    uint64_t* item_empty = item_full + kItemSlots;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const uint32_t lane = tid & 31;
+
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        for (int s = 0; s < kItemSlots; ++s) {
+            mbar_init(item_full + s, 1);
+            mbar_init(item_empty + s, 1);
+        }
+        fence_mbar_init();
+        sh.f.abort = 0;
+        sh.req = 0;
+        sh.arrived = 0;
+    }
+    __syncthreads();  // the only barrier the producer warp takes part in
+    if (warp == NCW) {
+        if (lane == 0) ws_producer<THREADS, J, STAGES, kScale>(p, ring, full, empty, item_full, item_empty, sh);
+        return;
+    }
+
+    // ---- consumer warps ----------------------------------------------------
+    const uint32_t lt = lanemask_lt();
+    const uint32_t cap = p.cap;
+    const uint32_t cap_s = p.cap - kRegionEntries;  // settled region [0, cap_s), then the warp regions
+    uint64_t* region = s_buf + cap_s + warp * R;
+    const uint32_t compact_at = cap - max(cap / 8, static_cast<uint32_t>(THREADS) + 8u);
+    const float4* ring4 = reinterpret_cast<const float4*>(ring);
+    uint32_t gbase = 0;  // ring index of the current item's first tile (same in every consumer warp)
+
+    for (uint32_t d = 0;; ++d) {
+        const uint32_t slot = d % kItemSlots;
+        if (tid == 0) {
+            int32_t w = p.nsegs;
+            if (ws_wait(item_full + slot, (d / kItemSlots) & 1u, &sh.f.abort, p.err)) w = sh.items[slot];
+            if (ld_volatile_u32(&sh.f.abort)) w = p.nsegs;
+            sh.cur = w;
+        }
+        block_sync<THREADS>();
+        const int32_t w = sh.cur;
+        if (w >= p.nsegs) break;
+        TaskView tv;
+        const SegGeom G = seg_geom<TW, kScale>(p, w, &tv);
+        if (!G.skip) {
+            const int t = G.sg.task;
+            const FusedTask& td = G.td;
+            const uint32_t k = tv.k;
+            const uint32_t mid_keep = k + (cap_s - k) / 2;
+            const bool multi = td.nseg > 1;
+            const float scaler = kScale ? task_scaler(tv.data, 0, tv.len, 1) : 0.0f;
+            const uint32_t pos0 = static_cast<uint32_t>(G.a0);
+            const uint32_t nvec = static_cast<uint32_t>(G.nvec);
+            const uint32_t ntiles = G.ntiles;
+            const uint32_t sample_r = ws_sample_rank(td, p.retry != 0);
+            const uint32_t ns = sample_r != 0 ? kSampleTiles : 0u;
+            const float4* gsrc = reinterpret_cast<const float4*>(tv.data + G.a0);
+            uint32_t wcnt = 0;  // entries in this warp's region (same in all its lanes)
+
+            for (int attempt = 0; attempt < 2; ++attempt) {
+                // attempt 0 streams the ring; attempt 1 (a single-segment task
+                // whose sampled threshold was too high) re-reads the segment
+                // from global memory with no threshold.
+                const bool from_ring = attempt == 0;
+                uint64_t thr = 0;
+                if (multi) {
+                    if (tid == 0) sh.thr = load_volatile_u64(p.gthr + t);
+                    block_sync<THREADS>();
+                    thr = sh.thr;
+                } else if (from_ring && ns != 0) {
+                    // The sample tiles come first: group maxima of 4 consecutive
+                    // samples, then the lower edge of the bin holding the
+                    // sample_r-th largest.
+                    uint64_t vor = 0, vand = ~0ull;
+                    const uint32_t s = (static_cast<uint32_t>(warp) + NCW - gbase % NCW) % NCW;  // my sample tile
+                    if (s < ns) {
+                        const uint32_t gt = gbase + s;
+                        const uint32_t st = gt % STAGES;
+                        const bool ok = ws_warp_wait(full + st, (gt / STAGES) & 1u, &sh.f.abort, p.err);
+                        const float4* src = ring4 + static_cast<size_t>(st) * TW4;
+#pragma unroll
+                        for (int j = 0; j < J; ++j) {
+                            const float4 f = ok ? src[j * 32 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+                            const uint32_t a = score_of<kScale>(__float_as_uint(f.x), scaler, tv.sp);
+                            const uint32_t b = score_of<kScale>(__float_as_uint(f.y), scaler, tv.sp);
+                            const uint32_t c = score_of<kScale>(__float_as_uint(f.z), scaler, tv.sp);
+                            const uint32_t e = score_of<kScale>(__float_as_uint(f.w), scaler, tv.sp);
+                            const uint64_t gm = static_cast<uint64_t>(max(max(a, b), max(c, e))) << 32;
+                            s_buf[s * TW4 + j * 32 + lane] = gm;
+                            vor |= gm;
+                            vand &= gm;
+                        }
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(empty + st);
+                    }
+                    block_or_and<THREADS>(vor, vand, sh.f.bs);  // barriers: the maxima are in s_buf
+                    const uint64_t kf =
+                        block_rank_threshold<THREADS>(s_buf, ns * TW4, sample_r, 4 * sample_r, vand, vor, sh.f.bs);
+                    thr = kf > 0 ? kf - 1 : 0ull;
+                }
+                block_sync<THREADS>();
+                if (tid == 0) {
+                    sh.f.cnt = 0;
+                    sh.thr = thr;
+                    sh.req = 0;
+                    sh.arrived = 0;
+                }
+                block_sync<THREADS>();
+                wcnt = 0;
+
+                // Head [s0, a0) and tail [a1, s1): fewer than 4 elements each (warp 0).
+                if (warp == 0) {
+                    const int nh = static_cast<int>(G.a0 - G.s0), nt = static_cast<int>(G.s1 - G.a1);
+                    bool pass = false;
+                    uint64_t c = 0;
+                    int64_t q = -1;
+                    if (tid < nh) q = G.s0 + tid;
+                    else if (tid >= 8 && tid - 8 < nt) q = G.a1 + (tid - 8);
+                    if (q >= 0) {
+                        const uint32_t bits = __float_as_uint(tv.data[q]);
+                        c = make_composite(score_of<kScale>(bits, scaler, tv.sp), static_cast<uint32_t>(q));
+                        pass = c > thr;
+                    }
+                    const uint32_t m = __ballot_sync(kFullMask, pass);
+                    if (pass) region[__popc(m & lt)] = c;
+                    wcnt = __popc(m);
+                }
+
+                FastFilter ff = make_fast_filter<kScale>(thr, tv.sp, scaler);
+                uint64_t gnext = 0;  // lane 0: latest global threshold, read a tile ahead of its use
+                // My data tiles: i = i0, i0 + NCW, ... (tile i is ring tile gbase + ns + i).
+                uint32_t i = (static_cast<uint32_t>(warp) + NCW - (gbase + ns) % NCW) % NCW;
+                uint32_t om = 0;     // element bits of tile i that found no room (tile i is held)
+                uint32_t mine = 0;   // my tiles done (threshold refresh cadence)
+                uint32_t polls = 0;
+                bool arrived_me = false;
+                for (;;) {
+                    if (__any_sync(kFullMask, ld_volatile_u32(&sh.req) != 0u)) {
+                        // Block-wide shrink: gather the regions, keep a few more
+                        // than k, raise the threshold; every consumer warp is here.
+                        block_sync<THREADS>();
+                        gather_regions<THREADS, R>(s_buf, cap_s, wcnt, sh.f);
+                        const uint64_t kf = shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh.f);
+                        if (tid == 0) {
+                            if (kf != 0 && kf - 1 > sh.thr) sh.thr = kf - 1;
+                            if (multi && kf != 0)
+                                atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), kf - 1);
+                            sh.req = 0;
+                        }
+                        block_sync<THREADS>();
+                        if (sh.thr > thr) {
+                            thr = sh.thr;
+                            ff = make_fast_filter<kScale>(thr, tv.sp, scaler);
+                        }
+                        if (__any_sync(kFullMask, om != 0u)) {
+                            // Place the rest of the held tile.
+                            const uint32_t gt = gbase + ns + i;
+                            const uint32_t st = gt % STAGES;
+                            const float4* src = from_ring ? ring4 + static_cast<size_t>(st) * TW4 : gsrc + i * TW4;
+                            const uint32_t qb = i * TW4;
+                            om = ws_place<J, kScale>(src, 0u, om, nvec - qb, qb, pos0, thr, ff, scaler, tv.sp, region,
+                                                     R, wcnt, lane);
+                            if (__any_sync(kFullMask, om != 0u)) {
+                                if (lane == 0) st_volatile_u32(&sh.req, 1u);
+                            } else {
+                                __syncwarp();
+                                if (from_ring && lane == 0) mbar_arrive(empty + st);
+                                i += NCW;
+                                ++mine;
+                            }
+                        }
+                        continue;
+                    }
+                    if (i < ntiles) {
+                        const uint32_t gt = gbase + ns + i;
+                        const uint32_t st = gt % STAGES;
+                        const float4* src;
+                        if (from_ring) {
+                            if (!__all_sync(kFullMask, mbar_try_wait(full + st, (gt / STAGES) & 1u))) {
+                                // Not there yet: poll again from the top of the loop,
+                                // which serves shrink requests (a requester may hold
+                                // the stage this tile needs).  Bounded.
+                                ++polls;
+                                if (__any_sync(kFullMask, polls >= kWaitPolls ||
+                                                              ((polls & 63u) == 0u &&
+                                                               ld_volatile_u32(&sh.f.abort) != 0u))) {
+                                    // The tile never came: the CTA aborts (the host
+                                    // reports the error word; results are void).
+                                    if (lane == 0) {
+                                        record_error(p.err, kErrTimeout);
+                                        st_volatile_u32(&sh.f.abort, 1u);
+                                    }
+                                    polls = 0;
+                                    i += NCW;
+                                }
+                                continue;
+                            }
+                            polls = 0;
+                            src = ring4 + static_cast<size_t>(st) * TW4;
+                        } else {
+                            src = gsrc + i * TW4;
+                        }
+                        const uint32_t qb = i * TW4;
+                        const uint32_t nv = nvec - qb < TW4 ? nvec - qb : TW4;
+                        const uint32_t gm = ws_group_mask<J, kScale>(src, nv, lane, ff, scaler);
+                        if (__any_sync(kFullMask, gm != 0u)) {
+                            om = ws_place<J, kScale>(src, gm, 0u, nv, qb, pos0, thr, ff, scaler, tv.sp, region, R,
+                                                     wcnt, lane);
+                            if (__any_sync(kFullMask, om != 0u)) {
+                                if (lane == 0) st_volatile_u32(&sh.req, 1u);
+                                continue;  // tile i stays held until its candidates are placed
+                            }
+                        }
+                        __syncwarp();
+                        if (from_ring && lane == 0) mbar_arrive(empty + st);
+                        i += NCW;
+                        ++mine;
+                        if (multi) {
+                            // Segments of the task raise a shared threshold: read it
+                            // every other tile and use it on the next one.
+                            if ((mine & 1u) == 1u) {
+                                if (lane == 0) gnext = load_volatile_u64(p.gthr + t);
+                            } else {
+                                const uint64_t gg = __shfl_sync(kFullMask, gnext, 0);
+                                if (gg > thr) {
+                                    thr = gg;
+                                    ff = make_fast_filter<kScale>(thr, tv.sp, scaler);
+                                }
+                            }
+                        }
+                        continue;
+                    }
+                    // All my tiles are done: wait (serving shrink requests) until
+                    // every consumer warp is done.
+                    if (!arrived_me) {
+                        arrived_me = true;
+                        if (lane == 0) atomicAdd(&sh.arrived, 1u);
+                    }
+                    if (__any_sync(kFullMask, ld_volatile_u32(&sh.arrived) >= static_cast<uint32_t>(NCW))) break;
+                    __nanosleep(32);
+                }
+                block_sync<THREADS>();
+                gather_regions<THREADS, R>(s_buf, cap_s, wcnt, sh.f);  // all candidates now in [0, sh.f.cnt)
+                if (!multi) {
+                    const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
+                    if (sh.f.cnt < want && from_ring && ns != 0) continue;  // sample too high: redo without it
+                }
+                break;
+            }
+            gbase += ns + ntiles;  // the ring tiles of this item (the redo reads global memory)
+
+            if (!multi) {
+                uint64_t kth = 0;
+                const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
+                const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
+                if (m != want && tid == 0) record_error(p.err, kErrInternal);
+                finish_task<THREADS, !kScale>(p, tv, s_buf, m < want ? m : want, sh.f);
+            } else {
+                // Multi-segment task: publish this segment's k-th composite, append
+                // the survivors to the task's candidate region, count the segment.
+                uint64_t kth = 0;
+                shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
+                if (tid == 0) {
+                    if (kth != 0) atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), kth - 1);
+                    sh.f.gthr = load_volatile_u64(p.gthr + t);
+                }
+                block_sync<THREADS>();
+                {
+                    const uint64_t gt = sh.f.gthr;
+                    const uint32_t cnt = sh.f.cnt;
+                    uint64_t* dst = p.cand + td.cbase;
+                    const uint32_t cregion = static_cast<uint32_t>(td.nseg) * p.kmax;
+                    for (uint32_t b0 = 0; b0 < cnt; b0 += THREADS) {
+                        const uint32_t ii = b0 + tid;
+                        const uint64_t c = (ii < cnt) ? s_buf[ii] : 0ull;
+                        const bool keep = (ii < cnt) && c > gt;
+                        uint32_t total;
+                        const uint32_t off = block_exclusive_scan<THREADS>(keep ? 1u : 0u, &total, sh.f.bs);
+                        if (tid == 0 && total) sh.f.base = atomicAdd(p.task_cnt + t, total);
+                        block_sync<THREADS>();
+                        if (keep) {
+                            const uint32_t o = sh.f.base + off;
+                            if (o < cregion) dst[o] = c;
+                            else record_error(p.err, kErrCapacity);
+                        }
+                        block_sync<THREADS>();
+                    }
+                }
+                __threadfence();
+                block_sync<THREADS>();
+                if (tid == 0) {
+                    const uint32_t done = atomicAdd(p.task_done + t, 1u);
+                    sh.f.last = (done == static_cast<uint32_t>(td.nseg - 1)) ? 1u : 0u;
+                }
+                block_sync<THREADS>();
+                if (sh.f.last) {
+                    // Last segment of the task: merge all segments' survivors.
+                    __threadfence();
+                    if (tid == 0) {
+                        sh.f.cnt = 0;
+                        sh.f.gthr = load_volatile_u64(p.gthr + t);
+                        sh.f.base = __ldcg(p.task_cnt + t);
+                    }
+                    block_sync<THREADS>();
+                    const uint64_t gt = sh.f.gthr;
+                    const uint32_t cregion = static_cast<uint32_t>(td.nseg) * p.kmax;
+                    const uint32_t n = sh.f.base < cregion ? sh.f.base : cregion;
+                    const unsigned long long* csrc = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
+                    for (uint32_t b0 = 0; b0 < n; b0 += THREADS) {
+                        {
+                            const uint32_t ii = b0 + tid;
+                            const uint64_t c = (ii < n) ? __ldcg(csrc + ii) : 0ull;
+                            warp_append((ii < n) && c > gt, c, s_buf, &sh.f.cnt, cap, p.err);
+                        }
+                        block_sync<THREADS>();
+                        const uint32_t cnt_now = sh.f.cnt;
+                        block_sync<THREADS>();
+                        if (cnt_now > compact_at) shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh.f);
+                    }
+                    block_sync<THREADS>();
+                    const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
+                    if (m < k && (td.flags & kTaskSampled) && !p.retry) {
+                        // The sampled threshold was above the task's k-th composite.
+                        if (tid == 0) p.fail[t] = 1u;
+                    } else {
+                        if (m != k && tid == 0) record_error(p.err, kErrInternal);
+                        finish_task<THREADS, !kScale>(p, tv, s_buf, m < k ? m : k, sh.f);
+                    }
+                }
+            }
+        }
+        block_sync<THREADS>();  // the item is finished: its slot may be reused
+        if (tid == 0) mbar_arrive(item_empty + slot);
+    }
+}
+
+}  // namespace radik

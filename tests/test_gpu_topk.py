@@ -216,3 +216,45 @@ def test_in_block_sample_redo(oracle, radik, torch_cuda):
     data = np.concatenate([x, x[::-1].copy()])
     for k in (64, 256, 1024):
         _compare(oracle, radik, torch_cuda, data, lens, k)
+
+
+KERNEL_FORMS = [{"RADIK_WS": "0"}, {"RADIK_WS": "1", "RADIK_WSJ": "8"}, {"RADIK_WS": "1", "RADIK_WSJ": "4"}]
+
+
+@pytest.mark.parametrize("form", KERNEL_FORMS, ids=["barrier", "ws-j8", "ws-j4"])
+def test_many_items_per_block(oracle, radik, torch_cuda, monkeypatch, form):
+    """A grid of 2-3 blocks works through every batch, so each block takes
+    many work items in a row: ring stages, phases and item slots carry over
+    from one item to the next, and a redo or a shrink in one item must not
+    disturb the next."""
+    for kk, vv in form.items():
+        monkeypatch.setenv(kk, vv)
+    monkeypatch.setenv("RADIK_GRID", "3")
+    rng = np.random.default_rng(77)
+    # sampled single-segment tasks (length >= 16384), several k
+    lens = [65536] * 12 + [20000, 16384, 40000, 3, 0, 70001]
+    x = rng.random(sum(lens), dtype=np.float32)
+    for k in (1, 64, 256, 1000):
+        _compare(oracle, radik, torch_cuda, x, lens, k)
+    _compare(oracle, radik, torch_cuda, x, lens, 100, largest=False, rev=True)
+    # 128 large values planted in sampled groups (32 chunks of 64 at multiples
+    # of 2048 for length 65536): the sampled threshold passes only those, fewer
+    # than k, so every other item takes the redo path
+    y = rng.random(65536 * 8, dtype=np.float32)
+    for t in range(0, 8, 2):
+        for c in range(32):
+            for off in (0, 4, 8, 12):
+                y[t * 65536 + c * 2048 + off] = 10.0 + rng.random(dtype=np.float32)
+    _compare(oracle, radik, torch_cuda, y, [65536] * 8, 256)
+    # uneven batch with custom indices
+    ulen = [int(v) for v in np.clip(rng.lognormal(np.log(5000), 1.3, size=60), 1, 200_000)]
+    z = rng.standard_normal(sum(ulen)).astype(np.float32)
+    ind = rng.permutation(sum(ulen)).astype(np.int32)
+    _compare(oracle, radik, torch_cuda, z, ulen, 64, indices=ind)
+    # multi-segment tasks (candidate regions, global thresholds, sampling)
+    monkeypatch.setenv("RADIK_SEG", "16384")
+    monkeypatch.setenv("RADIK_GRID", "2")
+    w = rng.standard_normal(1 << 20).astype(np.float32)
+    for k in (16, 256):
+        _compare(oracle, radik, torch_cuda, w, [1 << 20], k)
+        _compare(oracle, radik, torch_cuda, w, [300_000, 1 << 19, 5], k, largest=False)
