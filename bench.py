@@ -178,7 +178,8 @@ def profile_traffic(config: str):
     p = ROOT / "profiles" / "traffic.json"
     try:
         d = json.loads(p.read_text())
-        return d.get(config)
+        v = d.get(config)
+        return v if isinstance(v, (int, float)) else None
     except (OSError, ValueError):
         return None
 

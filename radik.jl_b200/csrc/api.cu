@@ -96,13 +96,14 @@ FusedKernel pick_fused(int threads, int vec, bool scale) {
 template <int NCW, int J, int ST, bool S>
 FusedKernel fused_ws_ptr() { return fused_ws_kernel<NCW, J, ST, S>; }
 
-FusedKernel pick_fused_ws(int threads, int j, bool scale) {
-    if (threads == 256 && j == 8) return scale ? fused_ws_ptr<8, 8, 16, true>() : fused_ws_ptr<8, 8, 16, false>();
-    if (threads == 256 && j == 4) return scale ? fused_ws_ptr<8, 4, 24, true>() : fused_ws_ptr<8, 4, 24, false>();
+// Shapes: consumer threads, float4 per lane in a warp tile (j), ring stages.
+FusedKernel pick_fused_ws(int threads, int j, int stages, bool scale) {
+    if (threads == 256 && j == 8 && stages == 16) return scale ? fused_ws_ptr<8, 8, 16, true>() : fused_ws_ptr<8, 8, 16, false>();
+    if (threads == 256 && j == 4 && stages == 24) return scale ? fused_ws_ptr<8, 4, 24, true>() : fused_ws_ptr<8, 4, 24, false>();
+    if (threads == 128 && j == 8 && stages == 8) return scale ? fused_ws_ptr<4, 8, 8, true>() : fused_ws_ptr<4, 8, 8, false>();
+    if (threads == 128 && j == 8 && stages == 12) return scale ? fused_ws_ptr<4, 8, 12, true>() : fused_ws_ptr<4, 8, 12, false>();
     return nullptr;
 }
-
-int ws_stages(int j) { return j == 8 ? 16 : 24; }
 
 // Dynamic shared memory of the fused kernel: TMA ring, candidate buffer,
 // one mbarrier per ring stage.
@@ -112,8 +113,8 @@ size_t fused_smem(uint32_t cap, int threads, int vec) {
 
 // Warp-specialised form: ring, candidate buffer, "full" and "empty" mbarrier
 // per stage, the item ring's barriers.
-size_t fused_ws_smem(uint32_t cap, int j) {
-    const size_t st = static_cast<size_t>(ws_stages(j));
+size_t fused_ws_smem(uint32_t cap, int j, int stages) {
+    const size_t st = static_cast<size_t>(stages);
     return st * 128 * j * sizeof(float) + static_cast<size_t>(cap) * 8 + (2 * st + 2 * kItemSlots) * 8;
 }
 
@@ -148,6 +149,9 @@ struct Plan {
     bool valid = false;
     bool fused = false;
     bool ws_form = false;   // warp-specialised fused kernel
+    int ws_stages = 16;     // its ring stages
+    int ws_sample_max = 2048;    // its single-segment sample (elements)
+    int ws_sample_windows = 2;   // digit windows of the sample's rank threshold
     int threads = 256, vec = 16;
     int launch_threads = 256;  // threads plus the producer warp of the warp-specialised form
     uint32_t cap = 0;
@@ -186,6 +190,7 @@ namespace {
 // Device state of one workspace.  The header holds the sticky error word and
 // the work counters; everything after `err` is zeroed before every call.
 struct StateLayout {
+    // kAny: multi-pass path: some task still active; fused path: some task failed.
     static constexpr size_t kErr = 0, kWork = 4, kWorkRetry = 8, kAny = 12, kHeader = 16;
     size_t gthr, gthr_r, done, done_r, cnt, cnt_r, fail, sdone, bytes;
     explicit StateLayout(int64_t T) {
@@ -234,22 +239,42 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     np.vec = env_int("RADIK_VEC", 8);
     const bool scale = (flags & RADIK_WITHSCALE) != 0;
     const size_t kk = static_cast<size_t>(k);
-    // Kernel form: the warp-specialised kernel (fused_ws.cuh) unless its
-    // larger ring leaves room for fewer than two blocks per SM, in which case
-    // the single-barrier form (fused.cuh) keeps more bytes in flight.
-    // RADIK_WS=0/1 forces a form.
+    // Kernel form: the warp-specialised kernel (fused_ws.cuh, 4 consumer
+    // warps and a producer warp, 8 warp tiles of 4 KB in its ring) when at
+    // least three blocks fit on an SM; otherwise the form that keeps more
+    // bytes in flight per SM (a large k makes the candidate buffer, not the
+    // ring, the larger part of shared memory).  RADIK_WS=0/1 forces a form;
+    // RADIK_WST / RADIK_WSJ / RADIK_WSS choose another shape of it.
     np.cap = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(np.threads) * np.vec, np.threads));
     const int ws_env = env_int("RADIK_WS", -1);
-    const int ws_j = env_int("RADIK_WSJ", 8);  // float4 per lane in a warp tile
-    np.ws_form = ws_env >= 0 ? ws_env != 0
-                             : (np.threads == 256 && 2 * (fused_ws_smem(np.cap, ws_j) + 2048) <=
-                                                         static_cast<size_t>(di.max_smem_optin));
-    if (np.ws_form) np.vec = ws_j;
-    FusedKernel fk = np.ws_form ? pick_fused_ws(np.threads, np.vec, scale) : pick_fused(np.threads, np.vec, scale);
+    const int ws_j = env_int("RADIK_WSJ", 8);           // float4 per lane in a warp tile
+    np.ws_stages = env_int("RADIK_WSS", 8);             // ring stages (a multiple of the consumer warps)
+    const int ws_threads = env_int("RADIK_WST", 128);   // consumer threads
+    np.ws_sample_max = env_int("RADIK_WS_SAMPLE", 2048);
+    np.ws_sample_windows = env_int("RADIK_WS_WINDOWS", 2);
+    if (np.ws_sample_max != 2048 && np.ws_sample_max != 4096) np.ws_sample_max = 2048;
+    {
+        const size_t sm_bytes = static_cast<size_t>(di.max_smem_optin) + 1024;  // per SM, a block's reserve included
+        const uint32_t ws_cap = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(ws_threads) * ws_j, ws_threads));
+        const size_t ws_blk = fused_ws_smem(ws_cap, ws_j, np.ws_stages) + 2048;
+        const size_t bar_blk = fused_smem(np.cap, np.threads, np.vec) + 2048;
+        const size_t ws_occ = std::min<size_t>(4, sm_bytes / ws_blk), bar_occ = std::min<size_t>(3, sm_bytes / bar_blk);
+        const size_t ws_ring = static_cast<size_t>(np.ws_stages) * 128 * ws_j * 4;
+        const size_t bar_ring = static_cast<size_t>(kStages) * np.threads * np.vec * 4;
+        const bool ws_auto = ws_occ >= 3 || (ws_occ >= 1 && ws_occ * ws_ring >= bar_occ * bar_ring);
+        np.ws_form = ws_env >= 0 ? ws_env != 0 : ws_auto;
+    }
+    if (np.ws_form) {
+        np.vec = ws_j;
+        np.threads = ws_threads;
+        np.cap = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(np.threads) * np.vec, np.threads));
+    }
+    FusedKernel fk = np.ws_form ? pick_fused_ws(np.threads, np.vec, np.ws_stages, scale)
+                                : pick_fused(np.threads, np.vec, scale);
     if (!fk) return fail(RADIK_ERR_INVALID, "unsupported RADIK_THREADS/RADIK_VEC combination");
     np.launch_threads = np.threads + (np.ws_form ? 32 : 0);
     const size_t tile = static_cast<size_t>(np.threads) * np.vec;
-    np.smem = np.ws_form ? fused_ws_smem(np.cap, np.vec) : fused_smem(np.cap, np.threads, np.vec);
+    np.smem = np.ws_form ? fused_ws_smem(np.cap, np.vec, np.ws_stages) : fused_smem(np.cap, np.threads, np.vec);
     np.fused = (flags & RADIK_PLAIN) == 0 && np.smem <= static_cast<size_t>(di.max_smem_optin) - 4096;
 
     int occ = 1;
@@ -305,8 +330,10 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
             const int64_t S = njobs * nchunks * kSampleChunk;
             const int64_t stride = (td.len / (njobs * nchunks)) & ~int64_t(3);
             const double lam = static_cast<double>(kk) * static_cast<double>(S) / static_cast<double>(td.len);
-            const int64_t r = static_cast<int64_t>(std::ceil(2.0 * lam + 4.0 * std::sqrt(lam) + 12.0));
-            if (allow_sample && nseg * static_cast<int64_t>(kk) >= 8192 && stride >= kSampleChunk && r <= 64) {
+            // Rank of the threshold among the sample's group maxima: lam + 3 sqrt(lam) + 6
+            // keeps the chance that fewer than k elements lie above it negligible.
+            const int64_t r = static_cast<int64_t>(std::ceil(lam + 3.0 * std::sqrt(lam) + 6.0));
+            if (allow_sample && nseg * static_cast<int64_t>(kk) >= 8192 && stride >= kSampleChunk + 4 && r <= 64) {
                 td.flags |= kTaskSampled;
                 for (int64_t j = 0; j < njobs; ++j) {
                     SampleJob sj;
@@ -440,6 +467,9 @@ FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, c
     p.task_done = ws->state.as<uint32_t>(L.done);
     p.task_cnt = ws->state.as<uint32_t>(L.cnt);
     p.fail = ws->state.as<uint32_t>(L.fail);
+    p.fail_any = ws->state.as<uint32_t>(StateLayout::kAny);
+    p.sample_max = static_cast<uint32_t>(pl.ws_sample_max);
+    p.sample_windows = static_cast<uint32_t>(pl.ws_sample_windows);
     p.cand = ws->cand.as<uint64_t>();
     p.sort_scratch = ws->scratch.as<uint64_t>();
     return p;
@@ -458,7 +488,8 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
             p, ws->desc.as<SampleJob>(pl.jobs_off), ws->samples.as<uint64_t>(), ws->state.as<uint32_t>(L.sdone));
         RADIK_CUDA(cudaGetLastError());
     }
-    FusedKernel fk = pl.ws_form ? pick_fused_ws(pl.threads, pl.vec, scale) : pick_fused(pl.threads, pl.vec, scale);
+    FusedKernel fk = pl.ws_form ? pick_fused_ws(pl.threads, pl.vec, pl.ws_stages, scale)
+                                : pick_fused(pl.threads, pl.vec, scale);
     fk<<<pl.grid, pl.launch_threads, pl.smem, s>>>(p);
     RADIK_CUDA(cudaGetLastError());
     if (!pl.jobs.empty()) {

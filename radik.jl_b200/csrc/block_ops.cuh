@@ -256,12 +256,12 @@ __device__ uint32_t block_shrink(uint64_t* buf, uint32_t cnt, uint32_t k, uint32
 }
 
 // Lower edge of the digit bin holding rank r (from the largest) among
-// buf[0, n) (unique composites inside [lo, hi]): at least r entries are >= it,
-// and at most about `slack` when two windows suffice.  The buffer is left as
-// it is.  All threads must call.
+// buf[0, n) (values inside [lo, hi]): at least r entries are >= it, and at
+// most `slack` unless `max_windows` digit windows do not get there.  The
+// buffer is left as it is.  All threads must call.
 template <int THREADS>
 __device__ uint64_t block_rank_threshold(const uint64_t* buf, uint32_t n, uint32_t r, uint32_t slack, uint64_t lo,
-                                         uint64_t hi, BlockScratch<THREADS>& s) {
+                                         uint64_t hi, BlockScratch<THREADS>& s, int max_windows = 2) {
     constexpr int W = 8;
     const int tid = threadIdx.x;
     const uint64_t diff = lo ^ hi;
@@ -271,7 +271,7 @@ __device__ uint64_t block_rank_threshold(const uint64_t* buf, uint32_t n, uint32
     int pbits = 63 - top;
     uint32_t above_total = 0;
     uint64_t keep_from = lo;
-    for (int pass = 0; pass < 2; ++pass) {
+    for (int pass = 0; pass < max_windows; ++pass) {
         const int w = top + 1 < W ? top + 1 : W;
         const int sh = top + 1 - w;
         const uint32_t nb = 1u << w;
@@ -313,6 +313,46 @@ __device__ uint32_t block_select_topk(uint64_t* buf, uint32_t cnt, uint32_t k, B
     uint32_t kept = block_shrink<THREADS>(buf, cnt, k, k, vand, vor, s, err, &kf, kth);
     if (cnt > k && kept != k && threadIdx.x == 0) record_error(err, kErrInternal);
     return kept;
+}
+
+// Ascending sort of buf[0, m) for m <= THREADS (unique keys below ~0):
+// every warp sorts 32 entries in registers (bitonic network over shuffles),
+// then each entry's final place is its lane plus, for every other warp's
+// sorted run, the number of entries below it (binary search).  Three
+// barriers in all; `runs` is scratch for THREADS entries.
+template <int THREADS>
+__device__ void small_sort_u64(uint64_t* buf, uint32_t m, uint64_t* runs) {
+    const int tid = threadIdx.x;
+    const uint32_t lane = tid & 31, warp = tid >> 5;
+    uint64_t v = static_cast<uint32_t>(tid) < m ? buf[tid] : ~0ull;
+#pragma unroll
+    for (uint32_t size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            const uint64_t o = __shfl_xor_sync(kFullMask, static_cast<unsigned long long>(v), stride);
+            const bool up = (lane & size) == 0;      // this block of `size` lanes ascends
+            const bool low = (lane & stride) == 0;   // lower lane of the pair
+            const bool take_min = low == up;
+            v = take_min ? (o < v ? o : v) : (o > v ? o : v);
+        }
+    }
+    runs[tid] = v;
+    block_sync<THREADS>();
+    uint32_t pos = lane;
+#pragma unroll
+    for (uint32_t w2 = 0; w2 < static_cast<uint32_t>(THREADS / 32); ++w2) {
+        if (w2 == warp) continue;
+        const uint64_t* r = runs + w2 * 32;
+        uint32_t c = 0;  // entries of run w2 below v
+#pragma unroll
+        for (uint32_t step = 16; step >= 1; step >>= 1)
+            if (r[c + step - 1] < v) c += step;
+        if (r[c] < v) ++c;
+        pos += c;
+    }
+    block_sync<THREADS>();
+    if (v != ~0ull && pos < m) buf[pos] = v;
+    block_sync<THREADS>();
 }
 
 // Bitonic sort of a[0, n) in shared memory (n a power of two), ascending or

@@ -80,6 +80,9 @@ struct FusedParams {
     uint32_t* task_done;     // [T] finished segments
     uint32_t* task_cnt;      // [T] entries in the candidate region
     uint32_t* fail;          // [T] seeded threshold too high
+    uint32_t* fail_any;      // [1] some task is flagged in `fail` (the retry launch exits at once otherwise)
+    uint32_t sample_max;     // warp-specialised kernel: most elements of a single-segment task's sample
+    uint32_t sample_windows; // digit windows of its rank threshold
     uint32_t* work_counter;  // [1]
     uint64_t* cand;          // candidate regions
     uint64_t* sort_scratch;  // [gridDim.x * kmax] (kmax > 4096 only)
@@ -232,7 +235,9 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
     }
     block_sync<THREADS>();
     uint64_t* sorted = buf;
-    if (m <= kBitonicMax) {
+    if (m <= static_cast<uint32_t>(THREADS) && p.cap >= 2u * THREADS) {
+        small_sort_u64<THREADS>(buf, m, buf + THREADS);
+    } else if (m <= kBitonicMax) {
         uint32_t P = 1;
         while (P < m) P <<= 1;
         for (uint32_t i = m + tid; i < P; i += THREADS) buf[i] = ~0ull;
@@ -331,6 +336,7 @@ constexpr uint32_t kRegionEntries = 2048;
 template <int THREADS, uint32_t R>
 __device__ void gather_regions(uint64_t* s_buf, uint32_t cap_s, uint32_t& wcnt, FusedShared<THREADS>& sh) {
     constexpr int NW = THREADS / 32;
+    constexpr uint32_t PER = (R + 31) / 32;  // region entries per lane
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t wc = wcnt < R ? wcnt : R;
     if (lane == 0) sh.wc[warp] = wc;
@@ -341,21 +347,20 @@ __device__ void gather_regions(uint64_t* s_buf, uint32_t cap_s, uint32_t& wcnt, 
         off += (i < warp) ? sh.wc[i] : 0u;
         total += sh.wc[i];
     }
-    // Warps move their entries one after another: warp w's destination ends
-    // at or before warp w+1's region, so no entry is overwritten unread.
-    for (int ww = 0; ww < NW; ++ww) {
-        if (sh.wc[ww] == 0) continue;  // same decision in every thread
-        if (warp == ww && off != cap_s + ww * R) {
-            const uint64_t* region = s_buf + cap_s + ww * R;
-            for (uint32_t base = 0; base < wc; base += 32) {
-                const uint32_t idx = base + lane;
-                const uint64_t x = idx < wc ? region[idx] : 0ull;
-                __syncwarp();
-                if (idx < wc) s_buf[off + idx] = x;
-                __syncwarp();
-            }
-        }
-        block_sync<THREADS>();
+    // Every warp takes its entries into registers first; a warp's destination
+    // may cover another warp's region, so nothing is written before all reads.
+    const uint64_t* region = s_buf + cap_s + warp * R;
+    uint64_t x[PER];
+#pragma unroll
+    for (uint32_t j = 0; j < PER; ++j) {
+        const uint32_t idx = j * 32 + lane;
+        x[j] = idx < wc ? region[idx] : 0ull;
+    }
+    block_sync<THREADS>();
+#pragma unroll
+    for (uint32_t j = 0; j < PER; ++j) {
+        const uint32_t idx = j * 32 + lane;
+        if (idx < wc) s_buf[off + idx] = x[j];
     }
     if (threadIdx.x == 0) sh.cnt = total;
     block_sync<THREADS>();
@@ -478,6 +483,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
     // Merge path (contiguous buffer): shrink once fewer than this many slots are free.
     const uint32_t compact_at = cap - max(cap / 8, static_cast<uint32_t>(THREADS) + 8u);
 
+    if (p.retry && *reinterpret_cast<volatile const uint32_t*>(p.fail_any) == 0u) return;  // nothing to redo
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) mbar_init(bars + s, 1);
         fence_mbar_init();
@@ -804,7 +810,10 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
                 const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh, &kth);
                 if (m < k && (td.flags & kTaskSampled) && !p.retry) {
                     // The sampled threshold was above the task's k-th composite.
-                    if (tid == 0) p.fail[t] = 1u;
+                    if (tid == 0) {
+                        p.fail[t] = 1u;
+                        atomicExch(p.fail_any, 1u);
+                    }
                 } else {
                     if (m != k && tid == 0) record_error(p.err, kErrInternal);
                     finish_task<THREADS, !kScale>(p, tv, s_buf, m < k ? m : k, sh);

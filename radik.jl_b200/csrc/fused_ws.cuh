@@ -81,32 +81,41 @@ __device__ __forceinline__ bool ws_warp_wait(uint64_t* bar, uint32_t parity, uin
     }
 }
 
-// Sample of a single-segment task: kSampleChunks chunks of kSampleChunkLen
-// consecutive elements spread evenly over the task (kSampleLen elements, the
-// first tiles of the task in the ring).  The consumers take the maximum score
-// of every 4 consecutive sampled elements (a group) and start from the lower
-// edge of the digit bin holding the r-th largest group maximum: at least r
-// groups, hence at least r sampled elements, score at or above it.  With
-// lam = k * kSampleLen / len sampled elements expected at or above the task's
-// k-th score, r = lam + 2 sqrt(lam) + 3 leaves a small chance (about 0.5% at
-// lam = 8) that the threshold is too high; the task is then recomputed
-// without it, so results never depend on the sample.  Returns r, or 0 when
-// the task gets no sample.
-constexpr uint32_t kSampleChunks = 32;
+// Sample of a single-segment task: chunks of kSampleChunkLen consecutive
+// elements spread evenly over the task (p.sample_max <= kSampleMax elements
+// for tasks of at least 16 times that, half as many down to 8 times the
+// half, none below; the first tiles of the task in the ring).  The consumers take the maximum
+// score of every 4 consecutive sampled elements (a group) and start from the
+// lower edge of the digit bin holding the r-th largest group maximum: at
+// least r groups, hence at least r sampled elements, score at or above it.
+// With lam = k * samples / len sampled elements expected at or above the
+// task's k-th score, r = lam + 2 sqrt(lam) + 3 leaves a small chance (about
+// 0.5% at lam = 8) that the threshold is too high; the task is then
+// recomputed without it, so results never depend on the sample.
 constexpr uint32_t kSampleChunkLen = 64;
-constexpr uint32_t kSampleLen = kSampleChunks * kSampleChunkLen;
+constexpr uint32_t kSampleMax = 4096;
 
-__device__ __forceinline__ uint32_t ws_sample_rank(const FusedTask& td, bool retry) {
-    if (retry || td.nseg != 1 || td.len < 8 * static_cast<int64_t>(kSampleLen)) return 0u;
-    const float lam = static_cast<float>(td.k) * static_cast<float>(kSampleLen) / static_cast<float>(td.len);
-    const uint32_t r = static_cast<uint32_t>(ceilf(lam + 2.0f * sqrtf(lam) + 3.0f));
-    return r <= kSampleLen / 4 / 4 ? r : 0u;  // at most a quarter of the groups
+// Sampled elements of a task (0: no sample); the same in producer and consumers.
+__device__ __forceinline__ uint32_t ws_sample_len(const FusedParams& p, const FusedTask& td) {
+    if (p.retry || td.nseg != 1) return 0u;
+    const uint32_t smax = p.sample_max;
+    if (td.len >= 16 * static_cast<int64_t>(smax)) return smax;
+    if (td.len >= 4 * static_cast<int64_t>(smax)) return smax / 2;
+    return 0u;
 }
 
-// First element of sample chunk c, 16-byte aligned in memory (mis: the task
-// pointer's offset in elements from a 16-byte boundary).
-__device__ __forceinline__ int64_t ws_sample_pos(int64_t len, int64_t mis, uint32_t c) {
-    int64_t q = ((static_cast<int64_t>(c) * len / kSampleChunks + mis) & ~int64_t(3)) - mis;
+// Rank r of the starting threshold among the sample's groups (0: none).
+__device__ __forceinline__ uint32_t ws_sample_rank(const FusedTask& td, uint32_t slen) {
+    if (slen == 0) return 0u;
+    const float lam = static_cast<float>(td.k) * static_cast<float>(slen) / static_cast<float>(td.len);
+    const uint32_t r = static_cast<uint32_t>(ceilf(lam + 2.0f * sqrtf(lam) + 3.0f));
+    return r <= slen / 4 / 4 ? r : 0u;  // at most a quarter of the groups
+}
+
+// First element of sample chunk c of nch, 16-byte aligned in memory (mis: the
+// task pointer's offset in elements from a 16-byte boundary).
+__device__ __forceinline__ int64_t ws_sample_pos(int64_t len, int64_t mis, uint32_t c, uint32_t nch) {
+    int64_t q = ((static_cast<int64_t>(c) * len / nch + mis) & ~int64_t(3)) - mis;
     if (q < 0) q += 4;
     const int64_t last = ((len - kSampleChunkLen + mis) & ~int64_t(3)) - mis;  // last aligned start that fits
     return q < last ? q : last;
@@ -117,9 +126,8 @@ template <int THREADS, int J, int STAGES, bool kScale>
 __device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, uint64_t* empty, uint64_t* item_full,
                             uint64_t* item_empty, WsShared<THREADS>& sh) {
     constexpr uint32_t TW = 128u * J;  // elements per warp tile
-    constexpr uint32_t kSampleTiles = kSampleLen / TW;
     constexpr uint32_t kChunksPerTile = TW / kSampleChunkLen;
-    static_assert(kSampleLen % TW == 0 && TW % kSampleChunkLen == 0, "sample tiles");
+    static_assert((kSampleMax / 2) % TW == 0 && TW % kSampleChunkLen == 0, "sample tiles");
     uint32_t g = 0;            // tiles issued
     uint32_t st = 0, eph = 1;  // stage of tile g; parity of the "empty" phase it must wait for
     for (uint32_t d = 0;; ++d) {
@@ -134,7 +142,9 @@ __device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, u
         const SegGeom G = seg_geom<TW, kScale>(p, w, &tv);
         if (G.skip) continue;
         bool ok = true;
-        const uint32_t ns = ws_sample_rank(G.td, p.retry != 0) != 0 ? kSampleTiles : 0u;
+        const uint32_t slen = ws_sample_len(p, G.td);
+        const uint32_t ns = ws_sample_rank(G.td, slen) != 0 ? slen / TW : 0u;
+        const uint32_t nch = slen / kSampleChunkLen;
         const uint32_t nt = G.ntiles + ns;
         const int64_t mis = static_cast<int64_t>((reinterpret_cast<uintptr_t>(tv.data) >> 2) & 3);
         for (uint32_t i = 0; i < nt; ++i, ++g) {
@@ -146,7 +156,7 @@ __device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, u
             if (i < ns) {
                 mbar_arrive_expect_tx(full + st, TW * 4u);
                 for (uint32_t c = 0; c < kChunksPerTile; ++c)
-                    bulk_load(dst + c * kSampleChunkLen, tv.data + ws_sample_pos(tv.len, mis, i * kChunksPerTile + c),
+                    bulk_load(dst + c * kSampleChunkLen, tv.data + ws_sample_pos(tv.len, mis, i * kChunksPerTile + c, nch),
                               kSampleChunkLen * 4u, full + st);
             } else {
                 const int64_t e0 = static_cast<int64_t>(i - ns) * TW;
@@ -263,11 +273,10 @@ __device__ __forceinline__ uint32_t ws_place(const float4* src, uint32_t groups,
 }
 
 template <int NCW, int J, int STAGES, bool kScale>
-__global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams p) {
+__global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_kernel(FusedParams p) {
     constexpr int THREADS = NCW * 32;             // consumer threads
     constexpr uint32_t TW = 128u * J;             // elements per warp tile (one ring stage)
     constexpr uint32_t TW4 = TW / 4;              // float4 per warp tile
-    constexpr uint32_t kSampleTiles = kSampleLen / TW;
     constexpr uint32_t R = kRegionEntries / NCW;  // append region of each consumer warp
     static_assert(J * 4 <= 32, "element bits of a lane fit in 32 bits");
     // Ring tile g sits in stage g % STAGES and belongs to warp g % NCW.  With
@@ -278,8 +287,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams
     // stages a warp could wait on phase n while phase n - 1, another warp's
     // tile, was still in flight, and the parity test would pass at once.)
     static_assert(STAGES % NCW == 0, "every ring stage belongs to one consumer warp");
-    static_assert(kSampleTiles <= static_cast<uint32_t>(NCW), "every sample tile has its own warp");
-    static_assert(kSampleLen / 4 <= kRegionEntries, "group maxima fit in the candidate buffer");
+    static_assert(kSampleMax / TW <= static_cast<uint32_t>(NCW), "every sample tile has its own warp");
+    static_assert(kSampleMax / 4 <= kRegionEntries, "group maxima fit in the candidate buffer");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ WsShared<THREADS> sh;
     float* ring = reinterpret_cast<float*>(smem_raw);
@@ -292,6 +301,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams
     const int warp = tid >> 5;
     const uint32_t lane = tid & 31;
 
+    if (p.retry && *reinterpret_cast<volatile const uint32_t*>(p.fail_any) == 0u) return;  // nothing to redo
     if (tid == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(full + s, 1);
@@ -344,28 +354,50 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams
             const uint32_t pos0 = static_cast<uint32_t>(G.a0);
             const uint32_t nvec = static_cast<uint32_t>(G.nvec);
             const uint32_t ntiles = G.ntiles;
-            const uint32_t sample_r = ws_sample_rank(td, p.retry != 0);
-            const uint32_t ns = sample_r != 0 ? kSampleTiles : 0u;
+            const uint32_t slen = ws_sample_len(p, td);
+            const uint32_t sample_r = ws_sample_rank(td, slen);
+            const uint32_t ns = sample_r != 0 ? slen / TW : 0u;
             const float4* gsrc = reinterpret_cast<const float4*>(tv.data + G.a0);
             uint32_t wcnt = 0;  // entries in this warp's region (same in all its lanes)
 
-            for (int attempt = 0; attempt < 2; ++attempt) {
-                // attempt 0 streams the ring; attempt 1 (a single-segment task
-                // whose sampled threshold was too high) re-reads the segment
-                // from global memory with no threshold.
+            bool thr_used = false;  // the last attempt started from a sampled threshold
+            for (int attempt = 0; attempt < 3; ++attempt) {
+                // attempt 0 streams the ring from the sample's threshold (rank
+                // sample_r).  A single-segment task whose threshold turned out
+                // too high re-reads the segment from global memory: attempt 1
+                // from a far more conservative rank of the same sample (read
+                // again from global memory), attempt 2 with no threshold.
                 const bool from_ring = attempt == 0;
                 uint64_t thr = 0;
+                thr_used = false;
                 if (multi) {
                     if (tid == 0) sh.thr = load_volatile_u64(p.gthr + t);
                     block_sync<THREADS>();
                     thr = sh.thr;
-                } else if (from_ring && ns != 0) {
-                    // The sample tiles come first: group maxima of 4 consecutive
-                    // samples, then the lower edge of the bin holding the
-                    // sample_r-th largest.
+                } else if (ns != 0 && attempt < 2) {
+                    // Group maxima of 4 consecutive samples, then the lower edge
+                    // of the bin holding the rr-th largest.
+                    const uint32_t rr = attempt == 0 ? sample_r : 4 * sample_r + 16;
+                    const uint32_t ngroups = slen / 4;
                     uint64_t vor = 0, vand = ~0ull;
                     const uint32_t s = (static_cast<uint32_t>(warp) + NCW - gbase % NCW) % NCW;  // my sample tile
-                    if (s < ns) {
+                    if (attempt == 1) {
+                        const int64_t mis = static_cast<int64_t>((reinterpret_cast<uintptr_t>(tv.data) >> 2) & 3);
+                        const uint32_t nch = slen / kSampleChunkLen;
+                        for (uint32_t gi = tid; gi < ngroups; gi += THREADS) {
+                            const uint32_t c = gi / (kSampleChunkLen / 4), e = gi % (kSampleChunkLen / 4);
+                            const float4 f = *reinterpret_cast<const float4*>(
+                                tv.data + ws_sample_pos(tv.len, mis, c, nch) + 4 * e);
+                            const uint32_t a = score_of<kScale>(__float_as_uint(f.x), scaler, tv.sp);
+                            const uint32_t b = score_of<kScale>(__float_as_uint(f.y), scaler, tv.sp);
+                            const uint32_t cc = score_of<kScale>(__float_as_uint(f.z), scaler, tv.sp);
+                            const uint32_t ee = score_of<kScale>(__float_as_uint(f.w), scaler, tv.sp);
+                            const uint64_t gm = static_cast<uint64_t>(max(max(a, b), max(cc, ee))) << 32;
+                            s_buf[gi] = gm;
+                            vor |= gm;
+                            vand &= gm;
+                        }
+                    } else if (s < ns) {
                         const uint32_t gt = gbase + s;
                         const uint32_t st = gt % STAGES;
                         const bool ok = ws_warp_wait(full + st, (gt / STAGES) & 1u, &sh.f.abort, p.err);
@@ -386,9 +418,13 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams
                         if (lane == 0) mbar_arrive(empty + st);
                     }
                     block_or_and<THREADS>(vor, vand, sh.f.bs);  // barriers: the maxima are in s_buf
-                    const uint64_t kf =
-                        block_rank_threshold<THREADS>(s_buf, ns * TW4, sample_r, 4 * sample_r, vand, vor, sh.f.bs);
-                    thr = kf > 0 ? kf - 1 : 0ull;
+                    if (rr <= ngroups / 2) {
+                        const uint64_t kf =
+                            block_rank_threshold<THREADS>(s_buf, ngroups, rr, p.sample_windows > 2 ? rr + rr / 2 + 2 : 4 * rr,
+                                                          vand, vor, sh.f.bs, static_cast<int>(p.sample_windows));
+                        thr = kf > 0 ? kf - 1 : 0ull;
+                        thr_used = thr != 0;
+                    }
                 }
                 block_sync<THREADS>();
                 if (tid == 0) {
@@ -535,7 +571,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams
                 gather_regions<THREADS, R>(s_buf, cap_s, wcnt, sh.f);  // all candidates now in [0, sh.f.cnt)
                 if (!multi) {
                     const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
-                    if (sh.f.cnt < want && from_ring && ns != 0) continue;  // sample too high: redo without it
+                    if (sh.f.cnt < want && thr_used) continue;  // threshold too high: redo from a lower one
                 }
                 break;
             }
@@ -613,7 +649,10 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 3) fused_ws_kernel(FusedParams
                     const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
                     if (m < k && (td.flags & kTaskSampled) && !p.retry) {
                         // The sampled threshold was above the task's k-th composite.
-                        if (tid == 0) p.fail[t] = 1u;
+                        if (tid == 0) {
+                            p.fail[t] = 1u;
+                            atomicExch(p.fail_any, 1u);
+                        }
                     } else {
                         if (m != k && tid == 0) record_error(p.err, kErrInternal);
                         finish_task<THREADS, !kScale>(p, tv, s_buf, m < k ? m : k, sh.f);

@@ -4,10 +4,13 @@
 // segments' own k-th values: a segment's k-th best is far below the task's.
 // Before the fused kernel runs, each such task is sampled by `njobs` CTAs:
 // every CTA reads `nchunks` chunks of kSampleChunk contiguous elements spread
-// over the task and keeps the exact top r of its sample (block_select_topk);
-// the last CTA of the task (atomic counter, no waiting) takes the exact r-th
-// best of the union and stores it, minus one, as the task's exclusive global
-// threshold.  About r * len / sample_size elements of the task lie above it;
+// over the task (16-byte aligned, so as float4), reduces every 4 consecutive
+// samples to their best score (a group maximum) and keeps the exact top r of
+// its groups; the last CTA of the task (atomic counter, no waiting) takes the
+// lower edge of the digit bin holding the r-th best of the union, rounded
+// down to a whole score, and stores it, minus one, as the task's exclusive
+// global threshold.  At least r groups, hence r sampled elements, score at
+// or above it, so about r * len / samples elements of the task lie above it;
 // r is chosen on the host so that this count exceeds k with a wide margin.
 // The fused kernel verifies the count; a task whose seeded threshold was too
 // high is recomputed without it (retry launch).
@@ -24,10 +27,10 @@ struct SampleJob {
     int32_t job_in_task;
     int32_t njobs;       // CTAs sampling this task
     int32_t r;           // sample rank (from the best) of the threshold, <= 64
-    int32_t nchunks;     // chunks per CTA
+    int32_t nchunks;     // chunks per CTA (a multiple of THREADS * 16 / kSampleChunk)
     int32_t pad_;
     int64_t pos0;        // position (inside the task) of this CTA's first chunk
-    int64_t stride;      // distance between consecutive chunks
+    int64_t stride;      // distance between consecutive chunks (a multiple of 4)
     int64_t out_base;    // first of the task's njobs * r slots in the sample buffer
 };
 
@@ -36,43 +39,68 @@ __global__ void __launch_bounds__(THREADS) sample_threshold_kernel(FusedParams p
                                                                     uint64_t* sample_out, uint32_t* sample_done) {
     extern __shared__ __align__(16) uint64_t s_buf[];
     __shared__ FusedShared<THREADS> sh;
+    constexpr uint32_t kChunk4 = kSampleChunk / 4;  // float4 per chunk
     const int tid = threadIdx.x;
     const SampleJob job = jobs[blockIdx.x];
     const int t = job.task;
     const FusedTask td = p.tasks[t];
     const TaskView tv = task_view<kScale>(p, t, td);
     const float scaler = kScale ? task_scaler(tv.data, 0, tv.len, 1) : 0.0f;
-    const uint32_t ns = static_cast<uint32_t>(job.nchunks) * kSampleChunk;
-    for (uint32_t i = tid; i < ns; i += THREADS) {
-        int64_t q = job.pos0 + static_cast<int64_t>(i / kSampleChunk) * job.stride + (i % kSampleChunk);
-        if (q >= tv.len) {  // the host keeps chunks inside the task
+    // Chunks start at 16-byte boundaries: positions move up by the task
+    // pointer's misalignment (the host leaves room for it).
+    const int64_t mis = static_cast<int64_t>((reinterpret_cast<uintptr_t>(tv.data) >> 2) & 3);
+    const int64_t shift = (4 - mis) & 3;
+    const uint32_t ngroups = static_cast<uint32_t>(job.nchunks) * kChunk4;
+    uint64_t vor = 0, vand = ~0ull;
+    for (uint32_t gi = tid; gi < ngroups; gi += THREADS) {
+        const uint32_t c = gi / kChunk4, e = gi % kChunk4;
+        int64_t q = job.pos0 + static_cast<int64_t>(c) * job.stride + shift + 4 * static_cast<int64_t>(e);
+        if (q + 4 > tv.len) {  // the host keeps chunks inside the task
             record_error(p.err, kErrBounds);
-            q = 0;
+            q = shift;
         }
-        uint32_t bits = __float_as_uint(tv.data[q]);
-        s_buf[i] = make_composite(score_of<kScale>(bits, scaler, tv.sp), static_cast<uint32_t>(q));
+        const float4 f = *reinterpret_cast<const float4*>(tv.data + q);  // (q + mis) % 4 == 0
+        const uint32_t a = score_of<kScale>(__float_as_uint(f.x), scaler, tv.sp);
+        const uint32_t b = score_of<kScale>(__float_as_uint(f.y), scaler, tv.sp);
+        const uint32_t cc = score_of<kScale>(__float_as_uint(f.z), scaler, tv.sp);
+        const uint32_t d = score_of<kScale>(__float_as_uint(f.w), scaler, tv.sp);
+        // Unique composite: best score of the group, then the group's number.
+        const uint64_t g = (static_cast<uint64_t>(max(max(a, b), max(cc, d))) << 32) |
+                           (static_cast<uint32_t>(job.job_in_task) * ngroups + gi);
+        s_buf[gi] = g;
+        vor |= g;
+        vand &= g;
     }
-    __syncthreads();
+    block_or_and<THREADS>(vor, vand, sh.bs);  // barriers: the groups are in s_buf
     const uint32_t r = static_cast<uint32_t>(job.r);
-    uint64_t kth = 0;
-    uint32_t kept = block_select_topk<THREADS>(s_buf, ns, r, sh.bs, p.err, &kth);
+    uint64_t kf = 0, mn = 0;
+    const uint32_t kept = block_shrink<THREADS>(s_buf, ngroups, r, r, vand, vor, sh.bs, p.err, &kf, &mn);
     uint64_t* out = sample_out + job.out_base + static_cast<int64_t>(job.job_in_task) * r;
     for (uint32_t i = tid; i < r; i += THREADS) out[i] = (i < kept) ? s_buf[i] : 0ull;
     __threadfence();
-    __syncthreads();
+    block_sync<THREADS>();
     if (tid == 0) sh.last = (atomicAdd(sample_done + t, 1u) == static_cast<uint32_t>(job.njobs - 1)) ? 1u : 0u;
-    __syncthreads();
+    block_sync<THREADS>();
     if (!sh.last) return;
     __threadfence();
     const uint32_t nall = static_cast<uint32_t>(job.njobs) * r;
     const unsigned long long* src = reinterpret_cast<const unsigned long long*>(sample_out + job.out_base);
-    for (uint32_t i = tid; i < nall; i += THREADS) s_buf[i] = __ldcg(src + i);
-    __syncthreads();
-    // Zero entries (sample CTAs with fewer than r values) never rank above a
-    // real composite, which is always > 0.
-    kept = block_select_topk<THREADS>(s_buf, nall, r, sh.bs, p.err, &kth);
-    if (tid == 0 && kept >= r && kth > 1)
-        atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), static_cast<unsigned long long>(kth - 1));
+    vor = 0;
+    vand = ~0ull;
+    for (uint32_t i = tid; i < nall; i += THREADS) {
+        const uint64_t g = __ldcg(src + i);
+        s_buf[i] = g;
+        vor |= g;
+        vand &= g;
+    }
+    block_or_and<THREADS>(vor, vand, sh.bs);
+    // Zero entries (CTAs with fewer than r groups) never rank above a real
+    // group, whose composite is > 0.  The lower edge of the bin of rank r is
+    // rounded down to its score: every element at or above that score passes.
+    const uint64_t edge = block_rank_threshold<THREADS>(s_buf, nall, r, 4 * r, vand, vor, sh.bs);
+    const uint64_t score = edge >> 32;
+    if (tid == 0 && score > 0)
+        atomicMax(reinterpret_cast<unsigned long long*>(p.gthr + t), static_cast<unsigned long long>((score << 32) - 1));
 }
 
 }  // namespace radik

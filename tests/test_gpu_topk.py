@@ -218,10 +218,17 @@ def test_in_block_sample_redo(oracle, radik, torch_cuda):
         _compare(oracle, radik, torch_cuda, data, lens, k)
 
 
-KERNEL_FORMS = [{"RADIK_WS": "0"}, {"RADIK_WS": "1", "RADIK_WSJ": "8"}, {"RADIK_WS": "1", "RADIK_WSJ": "4"}]
+KERNEL_FORMS = [
+    {"RADIK_WS": "0"},
+    {"RADIK_WS": "1", "RADIK_WST": "256", "RADIK_WSJ": "8", "RADIK_WSS": "16"},
+    {"RADIK_WS": "1", "RADIK_WST": "256", "RADIK_WSJ": "4", "RADIK_WSS": "24"},
+    {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "8"},
+    {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "12", "RADIK_WS_SAMPLE": "4096",
+     "RADIK_WS_WINDOWS": "3"},
+]
 
 
-@pytest.mark.parametrize("form", KERNEL_FORMS, ids=["barrier", "ws-j8", "ws-j4"])
+@pytest.mark.parametrize("form", KERNEL_FORMS, ids=["barrier", "ws-256-j8", "ws-256-j4", "ws-128-s8", "ws-128-s12"])
 def test_many_items_per_block(oracle, radik, torch_cuda, monkeypatch, form):
     """A grid of 2-3 blocks works through every batch, so each block takes
     many work items in a row: ring stages, phases and item slots carry over
