@@ -14,6 +14,7 @@
 #include "fused.cuh"
 #include "fused_ws.cuh"
 #include "general.cuh"
+#include "merge.cuh"
 #include "sample.cuh"
 #include "stages.cuh"
 
@@ -74,6 +75,7 @@ DeviceInfo device_info() {
 }
 
 size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+size_t round_down_entries(size_t n) { return n / 64 * 64; }
 
 // ---------------------------------------------------------------------------
 // Fused kernel dispatch
@@ -118,6 +120,13 @@ size_t fused_ws_smem(uint32_t cap, int j, int stages) {
     return st * 128 * j * sizeof(float) + static_cast<size_t>(cap) * 8 + (2 * st + 2 * kItemSlots) * 8;
 }
 
+using MergeKernel = void (*)(FusedParams, const int32_t*);
+constexpr int kMergeThreads = 1024;  // one block per flush-mode task
+
+MergeKernel pick_merge(bool scale) {
+    return scale ? merge_topk_kernel<kMergeThreads, true> : merge_topk_kernel<kMergeThreads, false>;
+}
+
 using SampleKernel = void (*)(FusedParams, const SampleJob*, uint64_t*, uint32_t*);
 
 SampleKernel pick_sample(bool scale) {
@@ -159,10 +168,18 @@ struct Plan {
     size_t smem = 0;
     int64_t T = 0, N = 0, cand_entries = 0, sample_entries = 0;
     int32_t nsegs = 0;
-    size_t tasks_off = 0, segs_off = 0, jobs_off = 0;
+    size_t tasks_off = 0, segs_off = 0, jobs_off = 0, merge_off = 0;
+    // Retry launch (barrier form, full candidate buffer) for sampled tasks.
+    uint32_t retry_cap = 0;
+    size_t retry_smem = 0;
+    int retry_grid = 0, retry_threads = 256, retry_vec = 8;
+    // Merge kernel for flush-mode tasks.
+    uint32_t merge_cap = 0;
+    size_t merge_smem = 0;
     std::vector<FusedTask> tasks;
     std::vector<FusedSeg> segs;
     std::vector<SampleJob> jobs;
+    std::vector<int32_t> merge_tasks;
 };
 
 struct radik_ws {
@@ -225,81 +242,25 @@ size_t fused_cap(size_t k, size_t tile, int threads) {
     return round_up(cap, 64);
 }
 
-// Host half of a launch plan: kernel configuration, segment table, sample
-// jobs and descriptor offsets.  Allocates no device memory.
-int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& np) {
-    const DeviceInfo di = device_info();
-    np.T = T;
-    np.N = 0;
-    for (int64_t t = 0; t < T; ++t) np.N += lens[t];
-
-    // Fused configuration.  The shared buffer holds k + one tile + headroom;
-    // when that does not fit in shared memory the multi-pass path runs.
-    np.threads = env_int("RADIK_THREADS", 256);
-    np.vec = env_int("RADIK_VEC", 8);
-    const bool scale = (flags & RADIK_WITHSCALE) != 0;
-    const size_t kk = static_cast<size_t>(k);
-    // Kernel form: the warp-specialised kernel (fused_ws.cuh, 4 consumer
-    // warps and a producer warp, 8 warp tiles of 4 KB in its ring) when at
-    // least three blocks fit on an SM; otherwise the form that keeps more
-    // bytes in flight per SM (a large k makes the candidate buffer, not the
-    // ring, the larger part of shared memory).  RADIK_WS=0/1 forces a form;
-    // RADIK_WST / RADIK_WSJ / RADIK_WSS choose another shape of it.
-    np.cap = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(np.threads) * np.vec, np.threads));
-    const int ws_env = env_int("RADIK_WS", -1);
-    const int ws_j = env_int("RADIK_WSJ", 8);           // float4 per lane in a warp tile
-    np.ws_stages = env_int("RADIK_WSS", 8);             // ring stages (a multiple of the consumer warps)
-    const int ws_threads = env_int("RADIK_WST", 128);   // consumer threads
-    np.ws_sample_max = env_int("RADIK_WS_SAMPLE", 2048);
-    np.ws_sample_windows = env_int("RADIK_WS_WINDOWS", 2);
-    if (np.ws_sample_max != 2048 && np.ws_sample_max != 4096) np.ws_sample_max = 2048;
-    {
-        const size_t sm_bytes = static_cast<size_t>(di.max_smem_optin) + 1024;  // per SM, a block's reserve included
-        const uint32_t ws_cap = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(ws_threads) * ws_j, ws_threads));
-        const size_t ws_blk = fused_ws_smem(ws_cap, ws_j, np.ws_stages) + 2048;
-        const size_t bar_blk = fused_smem(np.cap, np.threads, np.vec) + 2048;
-        const size_t ws_occ = std::min<size_t>(4, sm_bytes / ws_blk), bar_occ = std::min<size_t>(3, sm_bytes / bar_blk);
-        const size_t ws_ring = static_cast<size_t>(np.ws_stages) * 128 * ws_j * 4;
-        const size_t bar_ring = static_cast<size_t>(kStages) * np.threads * np.vec * 4;
-        const bool ws_auto = ws_occ >= 3 || (ws_occ >= 1 && ws_occ * ws_ring >= bar_occ * bar_ring);
-        np.ws_form = ws_env >= 0 ? ws_env != 0 : ws_auto;
-    }
-    if (np.ws_form) {
-        np.vec = ws_j;
-        np.threads = ws_threads;
-        np.cap = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(np.threads) * np.vec, np.threads));
-    }
-    FusedKernel fk = np.ws_form ? pick_fused_ws(np.threads, np.vec, np.ws_stages, scale)
-                                : pick_fused(np.threads, np.vec, scale);
-    if (!fk) return fail(RADIK_ERR_INVALID, "unsupported RADIK_THREADS/RADIK_VEC combination");
-    np.launch_threads = np.threads + (np.ws_form ? 32 : 0);
-    const size_t tile = static_cast<size_t>(np.threads) * np.vec;
-    np.smem = np.ws_form ? fused_ws_smem(np.cap, np.vec, np.ws_stages) : fused_smem(np.cap, np.threads, np.vec);
-    np.fused = (flags & RADIK_PLAIN) == 0 && np.smem <= static_cast<size_t>(di.max_smem_optin) - 4096;
-
-    int occ = 1;
-    if (np.fused) {
-        static std::mutex attr_mu;
-        {
-            std::lock_guard<std::mutex> lock(attr_mu);
-            cudaFuncSetAttribute(reinterpret_cast<const void*>(fk), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(np.smem));
-        }
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fk, np.launch_threads, np.smem) != cudaSuccess ||
-            occ < 1)
-            occ = 1;
-    }
-    const int64_t resident = static_cast<int64_t>(occ) * di.sms;
-
-    // Segments: tasks longer than seg_len are split (the last segment of a
-    // task may be shorter).
+// Segment length: about three work items per resident block, at least 64
+// tiles, a multiple of the tile (env RADIK_SEG overrides).
+int64_t pick_seg_len(int64_t N, int64_t resident, size_t tile, bool fused) {
     int64_t seg_len = env_int("RADIK_SEG", 0);
     if (seg_len <= 0) {
-        int64_t target = np.N / std::max<int64_t>(1, 3 * resident);
+        const int64_t target = N / std::max<int64_t>(1, 3 * resident);
         seg_len = std::max<int64_t>(64 * static_cast<int64_t>(tile), target);
     }
     seg_len = static_cast<int64_t>(round_up(static_cast<size_t>(seg_len), tile));
-    if (!np.fused) seg_len = std::max<int64_t>(seg_len, 1 << 20);
+    if (!fused) seg_len = std::max<int64_t>(seg_len, 1 << 20);
+    return seg_len;
+}
+
+// Splits the tasks into segments of seg_len (the fused path splits a task
+// only when it is longer than seg_len and than k) and decides which split
+// tasks are sampled: fills tasks, segs, jobs, cand_entries, sample_entries.
+void segment_tasks(Plan& np, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int64_t seg_len,
+                   bool fused) {
+    const size_t kk = static_cast<size_t>(k);
     np.tasks.resize(T);
     np.segs.clear();
     np.jobs.clear();
@@ -316,11 +277,11 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
         td.flags = tflags;
         td.pad_ = 0;
         int64_t nseg = 1;
-        if (np.fused && td.len > seg_len && td.len > k) nseg = (td.len + seg_len - 1) / seg_len;
-        if (!np.fused) nseg = std::max<int64_t>(1, (td.len + seg_len - 1) / seg_len);
+        if (fused && td.len > seg_len && td.len > k) nseg = (td.len + seg_len - 1) / seg_len;
+        if (!fused) nseg = std::max<int64_t>(1, (td.len + seg_len - 1) / seg_len);
         td.nseg = static_cast<int32_t>(nseg);
         td.cbase = -1;
-        if (np.fused && nseg > 1) {
+        if (fused && nseg > 1) {
             td.cbase = np.cand_entries;
             np.cand_entries += nseg * static_cast<int64_t>(kk);
             // Seed the global threshold from a sample when the segments' own
@@ -351,13 +312,13 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
                 np.sample_entries += njobs * r;
             }
         }
-        for (int64_t s = 0; s < nseg; ++s) {
+        for (int64_t sgi = 0; sgi < nseg; ++sgi) {
             FusedSeg sg;
-            sg.pos = static_cast<int32_t>(s * seg_len);
-            int64_t e = std::min(td.len, (s + 1) * seg_len);
-            sg.len = static_cast<int32_t>(e - s * seg_len);
+            sg.pos = static_cast<int32_t>(sgi * seg_len);
+            const int64_t e = std::min(td.len, (sgi + 1) * seg_len);
+            sg.len = static_cast<int32_t>(e - sgi * seg_len);
             sg.task = static_cast<int32_t>(t);
-            sg.seg_in_task = static_cast<int32_t>(s);
+            sg.seg_in_task = static_cast<int32_t>(sgi);
             np.segs.push_back(sg);
         }
         off += td.len;
@@ -366,18 +327,141 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     std::stable_sort(np.segs.begin(), np.segs.end(),
                      [](const FusedSeg& a, const FusedSeg& b) { return a.len > b.len; });
     np.nsegs = static_cast<int32_t>(np.segs.size());
+}
+
+// Sets a kernel's dynamic shared memory limit and returns how many of its
+// blocks fit on an SM (0 when it does not fit at all).
+int set_smem_and_occupancy(const void* fn, int threads, size_t smem) {
+    static std::mutex attr_mu;
+    std::lock_guard<std::mutex> lock(attr_mu);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return occ;
+}
+
+// Host half of a launch plan: kernel configuration, segment table, sample
+// jobs and descriptor offsets.  Allocates no device memory.
+int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& np) {
+    const DeviceInfo di = device_info();
+    np.T = T;
+    np.N = 0;
+    for (int64_t t = 0; t < T; ++t) np.N += lens[t];
+    const bool scale = (flags & RADIK_WITHSCALE) != 0;
+    const bool plain = (flags & RADIK_PLAIN) != 0;
+    const size_t kk = static_cast<size_t>(k);
+    const size_t smem_max = static_cast<size_t>(di.max_smem_optin) - 4096;
+
+    // Shapes.  Barrier form (fused.cuh): RADIK_THREADS x RADIK_VEC tiles.
+    // Warp-specialised form (fused_ws.cuh): RADIK_WST consumer threads,
+    // warp tiles of 128 * RADIK_WSJ elements, RADIK_WSS ring stages.
+    const int bar_threads = env_int("RADIK_THREADS", 256);
+    const int bar_vec = env_int("RADIK_VEC", 8);
+    const int ws_env = env_int("RADIK_WS", -1);
+    const int ws_j = env_int("RADIK_WSJ", 8);
+    const int ws_threads = env_int("RADIK_WST", 128);
+    np.ws_stages = env_int("RADIK_WSS", 8);
+    np.ws_sample_max = env_int("RADIK_WS_SAMPLE", 2048);
+    np.ws_sample_windows = env_int("RADIK_WS_WINDOWS", 2);
+    if (np.ws_sample_max != 2048 && np.ws_sample_max != 4096) np.ws_sample_max = 2048;
+    const size_t seg_tile = 2048;  // segments are whole tiles of either form
+
+    // Segments and samples first, sized for the warp-specialised form's
+    // residency (four blocks per SM).
+    segment_tasks(np, lens, T, k, flags, pick_seg_len(np.N, 4LL * di.sms, seg_tile, !plain), !plain);
+    bool all_flush = T > 0;  // every non-empty task is split and sampled
+    for (int64_t t = 0; t < T; ++t)
+        if (lens[t] > 0 && (np.tasks[t].flags & kTaskSampled) == 0) all_flush = false;
+
+    // Kernel form: the warp-specialised kernel when at least three of its
+    // blocks fit on an SM, else the form that keeps more bytes in flight per
+    // SM (a large k makes the candidate buffer the larger part of shared
+    // memory).  In the warp-specialised form, sampled split tasks run in
+    // flush mode and need no candidate buffer of k entries, so a batch made
+    // only of them gets the minimum buffer.  RADIK_WS=0/1 forces a form.
+    const uint32_t cap_bar = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(bar_threads) * bar_vec, bar_threads));
+    const uint32_t cap_ws = static_cast<uint32_t>(
+        fused_cap(all_flush ? 0 : kk, static_cast<size_t>(ws_threads) * ws_j, ws_threads));
+    {
+        const size_t sm_bytes = static_cast<size_t>(di.max_smem_optin) + 1024;  // per SM, a block's reserve included
+        const size_t ws_blk = fused_ws_smem(cap_ws, ws_j, np.ws_stages) + 2048;
+        const size_t bar_blk = fused_smem(cap_bar, bar_threads, bar_vec) + 2048;
+        const size_t ws_occ = std::min<size_t>(4, sm_bytes / ws_blk), bar_occ = std::min<size_t>(3, sm_bytes / bar_blk);
+        const size_t ws_ring = static_cast<size_t>(np.ws_stages) * 128 * ws_j * 4;
+        const size_t bar_ring = static_cast<size_t>(kStages) * bar_threads * bar_vec * 4;
+        const bool ws_auto = ws_occ >= 3 || (ws_occ >= 1 && ws_occ * ws_ring >= bar_occ * bar_ring);
+        np.ws_form = ws_env >= 0 ? ws_env != 0 : ws_auto;
+    }
+    np.threads = np.ws_form ? ws_threads : bar_threads;
+    np.vec = np.ws_form ? ws_j : bar_vec;
+    np.cap = np.ws_form ? cap_ws : cap_bar;
+    np.launch_threads = np.threads + (np.ws_form ? 32 : 0);
+    FusedKernel fk = np.ws_form ? pick_fused_ws(np.threads, np.vec, np.ws_stages, scale)
+                                : pick_fused(np.threads, np.vec, scale);
+    if (!fk) return fail(RADIK_ERR_INVALID, "unsupported RADIK_THREADS/RADIK_VEC/RADIK_WS* combination");
+    np.smem = np.ws_form ? fused_ws_smem(np.cap, np.vec, np.ws_stages) : fused_smem(np.cap, np.threads, np.vec);
+    np.fused = !plain && np.smem <= smem_max;
+    // Tasks that sample need the retry launch (barrier form, full buffer);
+    // flush-mode tasks need the merge kernel.
+    const bool sampled = !np.jobs.empty();
+    np.retry_cap = cap_bar;
+    np.retry_smem = fused_smem(cap_bar, bar_threads, bar_vec);
+    // The merge block takes nearly all of an SM's shared memory so that a
+    // task's whole candidate region (about 3k entries) usually fits at once.
+    np.merge_cap = static_cast<uint32_t>(
+        std::max(fused_cap(kk, 0, kMergeThreads), round_down_entries((smem_max - 8192) / 8)));
+    np.merge_smem = static_cast<size_t>(np.merge_cap) * 8;
+    if (np.fused && sampled && (np.retry_smem > smem_max || (np.ws_form && np.merge_smem > smem_max))) np.fused = false;
+
+    int occ = 1;
+    if (np.fused) {
+        occ = set_smem_and_occupancy(reinterpret_cast<const void*>(fk), np.launch_threads, np.smem);
+        if (occ < 1) np.fused = false;
+    }
+    if (!np.fused || !np.ws_form) {
+        // Re-segment for the form that runs.
+        occ = std::max(occ, 1);
+        segment_tasks(np, lens, T, k, flags, pick_seg_len(np.N, static_cast<int64_t>(occ) * di.sms, seg_tile, np.fused),
+                      np.fused);
+    }
+    const int64_t resident = static_cast<int64_t>(occ) * di.sms;
+    np.merge_tasks.clear();
+    if (np.fused && np.ws_form)
+        for (int64_t t = 0; t < T; ++t)
+            if (np.tasks[t].flags & kTaskSampled) {
+                np.tasks[t].flags |= kTaskFlush;
+                np.merge_tasks.push_back(static_cast<int32_t>(t));
+            }
     np.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(np.nsegs, resident)));
     const int grid_cap = env_int("RADIK_GRID", 0);  // fewer CTAs than resident (tests: many items per CTA)
     if (grid_cap > 0 && np.fused) np.grid = std::min(np.grid, grid_cap);
+    np.retry_grid = 0;
+    if (np.fused && !np.jobs.empty()) {
+        const int rocc = set_smem_and_occupancy(reinterpret_cast<const void*>(pick_fused(bar_threads, bar_vec, scale)),
+                                                bar_threads, np.retry_smem);
+        np.retry_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(np.nsegs, std::max(rocc, 1) * di.sms)));
+        if (grid_cap > 0) np.retry_grid = std::min(np.retry_grid, grid_cap);
+        np.retry_threads = bar_threads;
+        np.retry_vec = bar_vec;
+    }
+    if (np.fused && !np.merge_tasks.empty())
+        set_smem_and_occupancy(reinterpret_cast<const void*>(pick_merge(scale)), kMergeThreads, np.merge_smem);
     np.tasks_off = 0;
     np.segs_off = round_up(sizeof(FusedTask) * T, 256);
     np.jobs_off = np.segs_off + round_up(sizeof(FusedSeg) * np.segs.size(), 256);
+    np.merge_off = np.jobs_off + round_up(sizeof(SampleJob) * np.jobs.size(), 256);
     np.valid = true;
     return RADIK_OK;
 }
 
-// Size of the descriptor block (tasks, segments, sample jobs) of a plan.
-size_t plan_desc_bytes(const Plan& pl) { return pl.jobs_off + sizeof(SampleJob) * pl.jobs.size(); }
+// Size of the descriptor block (tasks, segments, sample jobs, merge list) of a plan.
+size_t plan_desc_bytes(const Plan& pl) { return pl.merge_off + sizeof(int32_t) * pl.merge_tasks.size(); }
 
 // Build the launch plan for a batch shape and size the workspace for it.
 int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes) {
@@ -404,8 +488,10 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     if (e == cudaSuccess && np.fused) {
         e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.cand_entries));
         if (e == cudaSuccess) e = ws->samples.ensure(sizeof(uint64_t) * static_cast<size_t>(np.sample_entries));
+        const size_t sort_blocks = std::max<size_t>(
+            {static_cast<size_t>(np.grid), static_cast<size_t>(np.retry_grid), np.merge_tasks.size()});
         if (e == cudaSuccess && kk > kBitonicMax)
-            e = ws->scratch.ensure(sizeof(uint64_t) * static_cast<size_t>(np.grid) * kk);
+            e = ws->scratch.ensure(sizeof(uint64_t) * sort_blocks * kk);
     }
     if (e == cudaSuccess && !np.fused) {
         e = ws->hist.ensure(sizeof(uint32_t) * 4096 * static_cast<size_t>(T));
@@ -427,6 +513,9 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !np.jobs.empty())
         e = cudaMemcpy(ws->desc.as<char>(np.jobs_off), np.jobs.data(), sizeof(SampleJob) * np.jobs.size(),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !np.merge_tasks.empty())
+        e = cudaMemcpy(ws->desc.as<char>(np.merge_off), np.merge_tasks.data(), sizeof(int32_t) * np.merge_tasks.size(),
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, L.bytes);
     if (e == cudaSuccess && np.fused && !np.jobs.empty()) {
@@ -492,16 +581,27 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
                                 : pick_fused(pl.threads, pl.vec, scale);
     fk<<<pl.grid, pl.launch_threads, pl.smem, s>>>(p);
     RADIK_CUDA(cudaGetLastError());
+    if (!pl.merge_tasks.empty()) {
+        // Flush-mode tasks: exact selection from their candidate regions.
+        FusedParams m = p;
+        m.cap = pl.merge_cap;
+        pick_merge(scale)<<<static_cast<unsigned>(pl.merge_tasks.size()), kMergeThreads, pl.merge_smem, s>>>(
+            m, ws->desc.as<int32_t>(pl.merge_off));
+        RADIK_CUDA(cudaGetLastError());
+    }
     if (!pl.jobs.empty()) {
-        // Recompute, without the sampled threshold, any task whose seeded
-        // threshold left fewer than k candidates; exits at once otherwise.
+        // Recompute, without the sampled threshold and with the full candidate
+        // buffer, any task whose seeded threshold left fewer than k candidates
+        // (or overflowed its region); exits at once otherwise.
         FusedParams r = p;
         r.retry = 1;
+        r.cap = pl.retry_cap;
         r.work_counter = ws->state.as<uint32_t>(StateLayout::kWorkRetry);
         r.gthr = ws->state.as<uint64_t>(L.gthr_r);
         r.task_done = ws->state.as<uint32_t>(L.done_r);
         r.task_cnt = ws->state.as<uint32_t>(L.cnt_r);
-        fk<<<pl.grid, pl.launch_threads, pl.smem, s>>>(r);
+        FusedKernel rk = pick_fused(pl.retry_threads, pl.retry_vec, scale);
+        rk<<<pl.retry_grid, pl.retry_threads, pl.retry_smem, s>>>(r);
         RADIK_CUDA(cudaGetLastError());
     }
     return RADIK_OK;
@@ -700,9 +800,10 @@ int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
     info->candidate_capacity = static_cast<int>(pl.cap);
     info->segments = pl.nsegs;
     info->sample_jobs = static_cast<int>(pl.jobs.size());
-    // fused: sampling kernel + fused kernel + retry launch when sampled;
+    // fused: sampling kernel + fused kernel (+ merge kernel for flush-mode
+    // tasks) + retry launch when sampled;
     // multi-pass: histogram, select, compact, advance, finalize at least.
-    info->kernels_per_call = pl.fused ? (pl.jobs.empty() ? 1 : 3) : 5;
+    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 1) : 5;
     return RADIK_OK;
 }
 
@@ -967,6 +1068,9 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
     if (!pl.jobs.empty())
         RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.jobs_off), pl.jobs.data(), sizeof(SampleJob) * pl.jobs.size(),
                                    cudaMemcpyHostToDevice, s));
+    if (!pl.merge_tasks.empty())
+        RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.merge_off), pl.merge_tasks.data(),
+                                   sizeof(int32_t) * pl.merge_tasks.size(), cudaMemcpyHostToDevice, s));
     FusedParams p = fused_params(&view, d_val_out, d_idx_out, idx_bytes, d_val_in, d_idx_in, k, flags);
     rc = run_fused(&view, p, flags, s);
     if (rc) return rc;

@@ -355,6 +355,80 @@ __device__ void small_sort_u64(uint64_t* buf, uint32_t m, uint64_t* runs) {
     block_sync<THREADS>();
 }
 
+// Ascending bitonic sort of n = THREADS * PER keys held in registers: thread
+// t holds elements t, t + THREADS, ...  A compare-exchange at stride s pairs
+// lanes of one warp (s < 32: shuffles), threads of different warps (32 <= s
+// < THREADS: through shared memory, two buffers `sm` of n entries each, one
+// barrier per stage) or registers of one thread (s >= THREADS).
+template <int THREADS, int PER>
+__device__ void bitonic_sort_regs(uint64_t (&v)[PER], uint64_t* sm) {
+    constexpr uint32_t N = THREADS * PER;
+    const uint32_t tid = threadIdx.x;
+    int buf = 0;
+    for (uint32_t size = 2; size <= N; size <<= 1) {
+        for (uint32_t s = size >> 1; s > 0; s >>= 1) {
+            if (s >= static_cast<uint32_t>(THREADS)) {
+                const uint32_t js = s / THREADS;
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+#pragma unroll
+                    for (int jp = j + 1; jp < PER; ++jp) {
+                        if (static_cast<uint32_t>(j ^ jp) == js) {
+                            const uint32_t e = static_cast<uint32_t>(j) * THREADS + tid;  // lower of the pair
+                            const bool up = (e & size) == 0;
+                            const uint64_t a = v[j], b = v[jp];
+                            const bool sw = up ? (a > b) : (a < b);
+                            v[j] = sw ? b : a;
+                            v[jp] = sw ? a : b;
+                        }
+                    }
+                }
+            } else if (s >= 32) {
+                uint64_t* x = sm + buf * N;
+#pragma unroll
+                for (int j = 0; j < PER; ++j) x[j * THREADS + tid] = v[j];
+                block_sync<THREADS>();
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                    const uint32_t e = static_cast<uint32_t>(j) * THREADS + tid;
+                    const uint64_t o = x[j * THREADS + (tid ^ s)];
+                    const bool up = (e & size) == 0, low = (tid & s) == 0;
+                    v[j] = (low == up) ? (o < v[j] ? o : v[j]) : (o > v[j] ? o : v[j]);
+                }
+                buf ^= 1;  // the next exchange writes the other buffer: no second barrier
+            } else {
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                    const uint32_t e = static_cast<uint32_t>(j) * THREADS + tid;
+                    const uint64_t o = __shfl_xor_sync(kFullMask, static_cast<unsigned long long>(v[j]), s);
+                    const bool up = (e & size) == 0, low = (tid & s) == 0;
+                    v[j] = (low == up) ? (o < v[j] ? o : v[j]) : (o > v[j] ? o : v[j]);
+                }
+            }
+        }
+    }
+    block_sync<THREADS>();  // the buffers may be reused
+}
+
+// Sorts buf[0, m) ascending with bitonic_sort_regs (n = THREADS * PER >= m,
+// padding ~0); scratch holds 2 n entries.
+template <int THREADS, int PER>
+__device__ void regs_sort_u64(uint64_t* buf, uint32_t m, uint64_t* scratch) {
+    uint64_t v[PER];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const uint32_t e = static_cast<uint32_t>(j) * THREADS + threadIdx.x;
+        v[j] = e < m ? buf[e] : ~0ull;
+    }
+    bitonic_sort_regs<THREADS, PER>(v, scratch);
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        const uint32_t e = static_cast<uint32_t>(j) * THREADS + threadIdx.x;
+        if (e < m) buf[e] = v[j];
+    }
+    block_sync<THREADS>();
+}
+
 // Bitonic sort of a[0, n) in shared memory (n a power of two), ascending or
 // descending.
 template <int THREADS>

@@ -35,7 +35,10 @@
 
 namespace radik {
 
-enum : uint32_t { kTaskLargest = 1u, kTaskAscend = 2u, kTaskSampled = 4u };
+// kTaskFlush: a sampled task split into segments whose candidates go straight
+// to its candidate region (no per-segment selection); the merge kernel
+// (merge.cuh) finishes it.
+enum : uint32_t { kTaskLargest = 1u, kTaskAscend = 2u, kTaskSampled = 4u, kTaskFlush = 8u };
 
 struct FusedTask {
     int64_t start;   // global offset of the task in p.data (uniform-input mode)
@@ -235,8 +238,16 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
     }
     block_sync<THREADS>();
     uint64_t* sorted = buf;
+    // Scratch past the entries for the register sorts: their n <= 8 THREADS
+    // keys need 2 n slots after buf[0, n).
     if (m <= static_cast<uint32_t>(THREADS) && p.cap >= 2u * THREADS) {
         small_sort_u64<THREADS>(buf, m, buf + THREADS);
+    } else if (m <= 2u * THREADS && p.cap >= 6u * THREADS) {
+        regs_sort_u64<THREADS, 2>(buf, m, buf + 2 * THREADS);
+    } else if (m <= 4u * THREADS && p.cap >= 12u * THREADS) {
+        regs_sort_u64<THREADS, 4>(buf, m, buf + 4 * THREADS);
+    } else if (THREADS <= 256 && m <= 8u * THREADS && p.cap >= 24u * THREADS) {
+        regs_sort_u64<THREADS, (THREADS <= 256 ? 8 : 1)>(buf, m, buf + 8 * THREADS);
     } else if (m <= kBitonicMax) {
         uint32_t P = 1;
         while (P < m) P <<= 1;

@@ -67,6 +67,29 @@ __device__ __forceinline__ bool ws_wait(uint64_t* bar, uint32_t parity, uint32_t
     return false;
 }
 
+// Appends a warp's region (its first min(wcnt, R) entries) to a task's
+// candidate region in global memory: one atomic per warp reserves the slots.
+// A region that would overflow flags the task (the retry launch recomputes
+// it) and is dropped.  All lanes of the warp must call; wcnt becomes 0.
+__device__ __forceinline__ void ws_flush(const uint64_t* region, uint32_t& wcnt, uint32_t R, uint64_t* dst,
+                                         uint32_t* cnt, uint32_t cap, uint32_t* fail_t, uint32_t* fail_any,
+                                         uint32_t lane) {
+    const uint32_t n = wcnt < R ? wcnt : R;
+    if (n != 0) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(cnt, n);
+        base = __shfl_sync(kFullMask, base, 0);
+        if (static_cast<uint64_t>(base) + n <= cap) {
+            for (uint32_t i = lane; i < n; i += 32) dst[base + i] = region[i];
+        } else if (lane == 0) {
+            *fail_t = 1u;
+            atomicExch(fail_any, 1u);
+        }
+        __syncwarp();
+    }
+    wcnt = 0;
+}
+
 // Bounded wait of a whole warp on one mbarrier phase.
 __device__ __forceinline__ bool ws_warp_wait(uint64_t* bar, uint32_t parity, uint32_t* abort, uint32_t* err) {
     for (uint32_t polls = 1;; ++polls) {
@@ -350,6 +373,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
             const uint32_t k = tv.k;
             const uint32_t mid_keep = k + (cap_s - k) / 2;
             const bool multi = td.nseg > 1;
+            // Flush mode: candidates above the seeded threshold go straight to the
+            // task's candidate region; no per-segment selection (merge.cuh finishes).
+            const bool flush = multi && (td.flags & kTaskFlush) != 0 && !p.retry;
+            uint64_t* fdst = p.cand + (td.cbase >= 0 ? td.cbase : 0);
+            const uint32_t fcap = static_cast<uint32_t>(td.nseg) * p.kmax;
             const float scaler = kScale ? task_scaler(tv.data, 0, tv.len, 1) : 0.0f;
             const uint32_t pos0 = static_cast<uint32_t>(G.a0);
             const uint32_t nvec = static_cast<uint32_t>(G.nvec);
@@ -534,7 +562,16 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                         if (__any_sync(kFullMask, gm != 0u)) {
                             om = ws_place<J, kScale>(src, gm, 0u, nv, qb, pos0, thr, ff, scaler, tv.sp, region, R,
                                                      wcnt, lane);
-                            if (__any_sync(kFullMask, om != 0u)) {
+                            if (flush) {
+                                // Write the region out and place the rest (bounded:
+                                // each round places up to R of at most 32 * 4 * J).
+                                for (int rounds = 0; rounds < 64 && __any_sync(kFullMask, om != 0u); ++rounds) {
+                                    ws_flush(region, wcnt, R, fdst, p.task_cnt + t, fcap, p.fail + t, p.fail_any,
+                                             lane);
+                                    om = ws_place<J, kScale>(src, 0u, om, nvec - qb, qb, pos0, thr, ff, scaler, tv.sp,
+                                                             region, R, wcnt, lane);
+                                }
+                            } else if (__any_sync(kFullMask, om != 0u)) {
                                 if (lane == 0) st_volatile_u32(&sh.req, 1u);
                                 continue;  // tile i stays held until its candidates are placed
                             }
@@ -561,6 +598,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                     // All my tiles are done: wait (serving shrink requests) until
                     // every consumer warp is done.
                     if (!arrived_me) {
+                        if (flush) ws_flush(region, wcnt, R, fdst, p.task_cnt + t, fcap, p.fail + t, p.fail_any, lane);
                         arrived_me = true;
                         if (lane == 0) atomicAdd(&sh.arrived, 1u);
                     }
@@ -568,6 +606,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                     __nanosleep(32);
                 }
                 block_sync<THREADS>();
+                if (flush) break;  // the candidates are in the task's region
                 gather_regions<THREADS, R>(s_buf, cap_s, wcnt, sh.f);  // all candidates now in [0, sh.f.cnt)
                 if (!multi) {
                     const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
@@ -577,7 +616,9 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
             }
             gbase += ns + ntiles;  // the ring tiles of this item (the redo reads global memory)
 
-            if (!multi) {
+            if (flush) {
+                // merge.cuh selects the task's k best from its candidate region.
+            } else if (!multi) {
                 uint64_t kth = 0;
                 const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
                 const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
