@@ -193,6 +193,9 @@ def run_reference(args, rank: int, world: int):
     if rank != 0:
         return
     oracle = load_oracle()
+    if args.config == "serving":
+        run_reference_serving(args, oracle, world)
+        return
     cfg = CONFIGS[args.config]
     lens = task_lens_of(args.config)
     threads = oracle.max_threads()
@@ -228,6 +231,36 @@ def run_reference(args, rank: int, world: int):
                 "restatement of its algorithm (oracle/) on the host cores",
     }
     print(json.dumps(line), flush=True)
+
+
+def run_reference_serving(args, oracle, world):
+    """CPU arm of the serving stream: the oracle port on the host cores,
+    requests served one after another, on a bounded sample (the first 6
+    requests of the stream, rows capped at 8)."""
+    rng = np.random.default_rng(4)
+    shapes = [(min(r, 8), l, k) for r, l, k in serving_requests(rng, 6)]
+    threads = oracle.max_threads()
+    data = np.random.default_rng(5).standard_normal(max(r * l for r, l, _ in shapes)).astype(np.float32)
+    for r, l, k in shapes[:1]:
+        oracle.topk(data[: r * l], [l] * r, min(k, l), largest=True, rev=False, threads=threads)
+    steps = max(args.steps, 1)
+    t0 = time.perf_counter()
+    elems = 0
+    for _ in range(steps):
+        for r, l, k in shapes:
+            oracle.topk(data[: r * l], [l] * r, min(k, l), largest=True, rev=False, threads=threads)
+            elems += r * l
+    dt = time.perf_counter() - t0
+    value = elems / dt
+    print(json.dumps({
+        "impl": "reference", "metric": "elements/s", "value": value, "unit": "elements/s", "n_gpus": world,
+        "steps": steps, "warmup": 1, "ms_per_step": dt * 1e3 / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "serving_stream"},
+        "cpu_baseline": {"value": value, "unit": "elements/s", "cores": threads, "kind": "port",
+                         "sample": "first 6 requests of the serving stream, rows capped at 8, served in order"},
+        "e2e": {"value": value, "unit": "elements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
 
 
 def cpu_baseline_quick(args) -> dict:
@@ -412,13 +445,122 @@ def run_ours(args, rank: int, world: int, dist):
     ws.close()
 
 
+# ---------------------------------------------------------------------------
+# Serving stream (request server, continuous batching)
+# ---------------------------------------------------------------------------
+SERVING_LOADS = (1000, 5000, 20000, 50000)  # offered requests per second
+SERVING_REQUESTS = 200                      # requests per offered load
+
+
+def serving_requests(rng, n):
+    """Request shapes of the serving stream: rows U{1..512}, row length from
+    {32768, 131072, 1048576}, k from {1, 50, 1024, 8192}."""
+    rows = rng.integers(1, 513, size=n)
+    lens = rng.choice([32768, 131072, 1048576], size=n)
+    ks = rng.choice([1, 50, 1024, 8192], size=n)
+    return [(int(r), int(l), int(k)) for r, l, k in zip(rows, lens, ks)]
+
+
+def run_serving(args, rank: int, world: int, dist):
+    """Poisson arrivals (seed 4) at each offered load; every request is a
+    [rows, row_len] slice of a device-resident pool of N(0,1) logits with a
+    Gumbel(0,1) tail on 1% of entries, k largest per row.  The server packs
+    requests into fused launches on 4 slots under a 32 GB admission cap.
+    Reported per load: achieved requests/s and elements/s, p50/p99 latency
+    from submission to completion; beside it the same arrival schedule served
+    one request at a time by the plain per-call path (the reference's launch
+    structure, workspace reused)."""
+    import torch
+    radik = load_package()
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(4 + rank)
+    pool_n = 1 << 29  # 2 GiB of logits: the largest request (512 x 2^20) fits
+    pool = torch.randn(pool_n, device="cuda", generator=g)
+    tail = torch.rand(pool_n, device="cuda", generator=g) < 0.01
+    u = torch.rand(pool_n, device="cuda", generator=g).clamp_(1e-12, 1.0)
+    pool += torch.where(tail, -torch.log(-torch.log(u)), torch.zeros_like(u))
+    del tail, u
+    rng = np.random.default_rng(4)
+    results = []
+    clocks = ClockSampler(local)
+    clocks.start()
+    with radik.Server(slots=4, mem_cap_bytes=32 << 30, max_batch_rows=4096) as srv:
+        # warm the slots' workspaces on every shape class
+        for r, l, k in [(4, 32768, 1), (4, 131072, 50), (2, 1048576, 1024), (2, 131072, 8192)]:
+            srv.wait(srv.submit(pool[: r * l].view(r, l), k), timeout_s=120)
+        for load in SERVING_LOADS:
+            shapes = serving_requests(rng, SERVING_REQUESTS)
+            gaps = rng.exponential(1.0 / load, size=len(shapes))
+            offs = [int(rng.integers(0, (pool_n - r * l) // 4 + 1)) * 4 for r, l, _ in shapes]
+            outs = [(torch.empty((r, k), device="cuda"), torch.empty((r, k), dtype=torch.int32, device="cuda"))
+                    for r, _, k in shapes]
+            torch.cuda.synchronize()
+            srv.reset_stats()
+            t0 = time.perf_counter()
+            due = t0
+            tickets = []
+            for (r, l, k), off, gap, (vo, io) in zip(shapes, offs, gaps, outs):
+                due += gap
+                while time.perf_counter() < due:
+                    pass
+                tickets.append(srv.submit(pool[off: off + r * l].view(r, l), k, val_out=vo, idx_out=io))
+            for t in tickets:
+                srv.wait(t, timeout_s=300)
+            dt = time.perf_counter() - t0
+            st = srv.stats()
+            elems = sum(r * l for r, l, _ in shapes)
+            # plain per-call path on the same schedule, one request at a time
+            ws = radik.RadiKWorkspace("cuda", 1 << 20, 512)
+            lat = []
+            t1 = time.perf_counter()
+            due = t1
+            for (r, l, k), off, gap, (vo, io) in zip(shapes, offs, gaps, outs):
+                due += gap
+                now = time.perf_counter()
+                if now < due:
+                    while time.perf_counter() < due:
+                        pass
+                radik.topk_radix_select_(vo, io, ws, pool[off: off + r * l], None, [l] * r, k, True, True,
+                                         plain=True)
+                lat.append((time.perf_counter() - due) * 1e6)
+            pdt = time.perf_counter() - t1
+            ws.close()
+            lat.sort()
+            results.append({
+                "offered_req_s": load, "requests": len(shapes), "elements": elems,
+                "served": {"req_s": len(shapes) / dt, "elements_s": elems / dt, "p50_us": st["p50_us"],
+                           "p99_us": st["p99_us"], "batches": st["batches"]},
+                "plain_per_call": {"req_s": len(shapes) / pdt, "elements_s": elems / pdt,
+                                   "p50_us": lat[len(lat) // 2], "p99_us": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            })
+    clk = clocks.stop()
+    if rank == 0:
+        best = max(results, key=lambda r: r["served"]["elements_s"])
+        line = {
+            "metric": "elements/s", "value": best["served"]["elements_s"] * world, "unit": "elements/s",
+            "n_gpus": world, "steps": len(SERVING_LOADS) * SERVING_REQUESTS, "warmup": 4,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "serving_stream", "loads_req_s": list(SERVING_LOADS),
+                       "requests_per_load": SERVING_REQUESTS, "slots": 4, "mem_cap_bytes": 32 << 30,
+                       "rows": "U{1..512}", "row_len": [32768, 131072, 1048576], "k": [1, 50, 1024, 8192],
+                       "arrivals": "Poisson, seed 4", "parallelism": f"replicas x{world}"},
+            "serving": results, "clocks": clk,
+            # each packed batch launches at least one kernel (sampling, merge and retry add more)
+            "gpu_launches": int(sum(r["served"]["batches"] for r in results)),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="uniform_batch", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="uniform_batch", choices=sorted(CONFIGS) + ["serving"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -438,7 +580,10 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     try:
-        run_ours(args, rank, world, dist)
+        if args.config == "serving":
+            run_serving(args, rank, world, dist)
+        else:
+            run_ours(args, rank, world, dist)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -138,6 +138,47 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
                        const void* d_idx_in, const int64_t* h_task_lens, int64_t num_tasks, int64_t k,
                        uint32_t flags, void* stream);
 
+/* ---- Request server (engine-specific, no reference counterpart) ----------
+ * Continuous batching of top-k requests: a worker thread packs pending
+ * requests that share (k, flags, index width) into one fused launch (every
+ * row of every request is a task with its own input and output pointers),
+ * runs up to `slots` launches at once on their own streams and device-
+ * resident workspaces, and admits a request only while the bytes of the
+ * requests in flight (inputs and outputs) plus the workspace pool stay under
+ * mem_cap_bytes.  Inputs and outputs are caller-owned device memory and must
+ * stay valid until the request completes. */
+typedef struct radik_server radik_server;
+
+typedef struct radik_server_config {
+    int slots;              /* concurrent launches (streams + workspaces), 1..64 */
+    int device;             /* CUDA device ordinal */
+    int64_t mem_cap_bytes;  /* admission cap: in-flight request bytes + workspace pool */
+    int64_t max_batch_rows; /* most rows packed into one launch */
+} radik_server_config;
+
+typedef struct radik_server_stats {
+    uint64_t submitted, completed, batches, rows;
+    double elements;        /* input elements of the completed requests */
+    double p50_us, p99_us, mean_us;  /* submit-to-completion latency of completed requests */
+    int64_t mem_in_flight;  /* request bytes in flight now */
+    int64_t mem_pool;       /* device bytes held by the slots' workspaces */
+} radik_server_stats;
+
+int radik_server_create(const radik_server_config* cfg, radik_server** server);
+/* Waits for every submitted request, then releases the server. */
+int radik_server_destroy(radik_server* server);
+/* Queues a request: d_data [rows][row_len] Float32 (row-major), outputs
+ * d_val_out [rows][k] and d_idx_out [rows][k] (idx_bytes wide, 1-based
+ * positions inside the row), flags RADIK_LARGEST / RADIK_ASCEND /
+ * RADIK_WITHSCALE as for radik_topk_radix_select.  *ticket identifies it. */
+int radik_server_submit(radik_server* server, const float* d_data, int64_t rows, int64_t row_len, int64_t k,
+                        uint32_t flags, float* d_val_out, void* d_idx_out, int idx_bytes, uint64_t* ticket);
+/* Waits up to timeout_us (negative: no limit) for a request; RADIK_OK when
+ * it completed (the ticket is then released), RADIK_ERR_TIMEOUT if not yet. */
+int radik_server_wait(radik_server* server, uint64_t ticket, int64_t timeout_us);
+int radik_server_get_stats(radik_server* server, radik_server_stats* stats);
+int radik_server_reset_stats(radik_server* server);
+
 /* ---- Stage entry points: the reference kernels' own contracts ----------- */
 
 /* count_bin_ex_kernel!, src/kernels/count_bin.jl:78-203: per-task histogram

@@ -29,7 +29,7 @@ from ._lib import (RADIK_ASCEND, RADIK_ASYNC, RADIK_LARGEST, RADIK_PLAIN, RADIK_
                    RADIK_WITHPACKING, RADIK_WITHSCALE, RadiKError, check, load)
 
 __all__ = ["topk", "topk_", "topk_radix_select_", "RadiKWorkspace", "RadiKError", "topk_host",
-           "count_bin_ex", "count_bin", "select_bin", "filter_", "version"]
+           "count_bin_ex", "count_bin", "select_bin", "filter_", "version", "Server"]
 
 
 def _torch():
@@ -360,3 +360,83 @@ def filter_(data, task_lens, kth, boundary, k: int, withscale=False, largest=Tru
     c = cnt.cpu().numpy()
     v, i = vo.cpu().numpy(), io.cpu().numpy()
     return [(v[t, :c[t]], i[t, :c[t]]) for t in range(T)], bnd.cpu().numpy()
+
+
+class Server:
+    """Request server over the C ABI (radik_server_*, include/radik.h):
+    continuous batching of top-k requests on a pool of ``slots`` streams
+    with device-resident workspaces, admission by memory (``mem_cap_bytes``
+    covers the inputs and outputs of the requests in flight plus the pool)
+    and latency statistics.  No counterpart in the reference, which serves
+    one call at a time."""
+
+    def __init__(self, slots: int = 4, mem_cap_bytes: int = 32 << 30, max_batch_rows: int = 4096, device=None):
+        torch = _torch()
+        from ._lib import ServerConfig
+        dev = torch.cuda.current_device() if device is None else int(device)
+        cfg = ServerConfig(int(slots), dev, int(mem_cap_bytes), int(max_batch_rows))
+        h = ctypes.c_void_p()
+        with torch.cuda.device(dev):
+            check(load().radik_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._keep = {}  # ticket -> tensors that must outlive the request
+
+    def submit(self, data, k: int, *, largest: bool = True, rev: bool = False, withscale: bool = False,
+               val_out=None, idx_out=None, idx_dtype=None) -> int:
+        """Queue ``data`` ((rows, row_len) CUDA Float32, row-major): the k best
+        of every row, sorted ascending unless ``rev`` (ASCEND = !rev as in
+        topk!).  Returns a ticket; outputs are (rows, k) tensors."""
+        torch = _torch()
+        _check_cuda(data, "data")
+        _check_float32(data)
+        if data.dim() == 1:
+            data = data.view(1, -1)
+        rows, row_len = data.shape
+        it = idx_dtype or torch.int32
+        if val_out is None:
+            val_out = torch.empty((rows, k), dtype=torch.float32, device=data.device)
+        if idx_out is None:
+            idx_out = torch.empty((rows, k), dtype=it, device=data.device)
+        flags = _flags(largest, not rev, withscale, False)
+        t = ctypes.c_uint64()
+        check(load().radik_server_submit(self._h, _ptr(data), rows, row_len, int(k), flags, _ptr(val_out),
+                                         _ptr(idx_out), _idx_bytes(idx_out.dtype), ctypes.byref(t)))
+        self._keep[t.value] = (data, val_out, idx_out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float | None = None):
+        """Block until the request completes; returns its (values, indices)."""
+        us = -1 if timeout_s is None else int(timeout_s * 1e6)
+        rc = load().radik_server_wait(self._h, ctypes.c_uint64(ticket), us)
+        if rc == 6:  # RADIK_ERR_TIMEOUT
+            raise TimeoutError(f"request {ticket} not complete")
+        keep = self._keep.pop(ticket, None)
+        check(rc)
+        return keep[1], keep[2]
+
+    def stats(self) -> dict:
+        from ._lib import ServerStats
+        st = ServerStats()
+        check(load().radik_server_get_stats(self._h, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in ServerStats._fields_}
+
+    def reset_stats(self) -> None:
+        check(load().radik_server_reset_stats(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            load().radik_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

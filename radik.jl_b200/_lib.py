@@ -33,6 +33,8 @@ EXPORTS = (
     "radik_topk_radix_select", "radik_topk", "radik_topk_host", "radik_topk_noalloc",
     "radik_count_bin_ex", "radik_count_bin", "radik_select_bin", "radik_filter",
     "radik_last_error", "radik_status_string", "radik_version",
+    "radik_server_create", "radik_server_destroy", "radik_server_submit", "radik_server_wait",
+    "radik_server_get_stats", "radik_server_reset_stats",
 )
 
 
@@ -41,6 +43,20 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "path", "block_threads", "grid", "smem_bytes", "candidate_capacity", "segments", "sample_jobs",
         "kernels_per_call")]
+
+
+class ServerConfig(ctypes.Structure):
+    """radik_server_config (include/radik.h)."""
+    _fields_ = [("slots", ctypes.c_int), ("device", ctypes.c_int), ("mem_cap_bytes", ctypes.c_int64),
+                ("max_batch_rows", ctypes.c_int64)]
+
+
+class ServerStats(ctypes.Structure):
+    """radik_server_stats (include/radik.h)."""
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("rows", ctypes.c_uint64), ("elements", ctypes.c_double), ("p50_us", ctypes.c_double),
+                ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("mem_in_flight", ctypes.c_int64),
+                ("mem_pool", ctypes.c_int64)]
 
 
 class RadiKError(Exception):
@@ -72,6 +88,12 @@ def _declare(L: ctypes.CDLL) -> None:
     L.radik_count_bin.argtypes = [P, P, P, I64, I64, I, I, P]
     L.radik_select_bin.argtypes = [P, P, P, P, I64, I64, I, P]
     L.radik_filter.argtypes = [P, P, I, P, P, P, P, P, P, I64, I64, I, I, P]
+    L.radik_server_create.argtypes = [ctypes.POINTER(ServerConfig), PP]
+    L.radik_server_destroy.argtypes = [P]
+    L.radik_server_submit.argtypes = [P, P, I64, I64, I64, U32, P, P, I, ctypes.POINTER(ctypes.c_uint64)]
+    L.radik_server_wait.argtypes = [P, ctypes.c_uint64, I64]
+    L.radik_server_get_stats.argtypes = [P, ctypes.POINTER(ServerStats)]
+    L.radik_server_reset_stats.argtypes = [P]
     L.radik_last_error.restype = ctypes.c_char_p
     L.radik_status_string.restype = ctypes.c_char_p
     L.radik_status_string.argtypes = [I]

@@ -189,6 +189,8 @@ struct radik_ws {
     int index_bytes = 4;
     cudaStream_t last_stream = nullptr;
     uint32_t* h_err = nullptr;  // pinned
+    char* h_stage = nullptr;    // pinned staging of plan descriptors (stream-ordered uploads)
+    size_t h_stage_bytes = 0;
     DevBuf state;     // StateLayout: per-call counters and thresholds
     DevBuf desc;      // tasks + segs + sample jobs of the plan
     DevBuf cand;      // fused: candidate regions of multi-segment tasks
@@ -464,7 +466,11 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
 size_t plan_desc_bytes(const Plan& pl) { return pl.merge_off + sizeof(int32_t) * pl.merge_tasks.size(); }
 
 // Build the launch plan for a batch shape and size the workspace for it.
-int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes) {
+// With `upload` set, descriptors are uploaded with copies ordered on that
+// stream from pinned staging memory (the request server: no host wait, no
+// legacy-stream synchronisation); otherwise synchronously.
+int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes,
+               cudaStream_t upload = nullptr, bool use_upload = false) {
     Plan& pl = ws->plan;
     PlanKey key;
     key.lens.assign(lens, lens + T);
@@ -507,17 +513,40 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
         return fail(e == cudaErrorMemoryAllocation ? RADIK_ERR_OOM : RADIK_ERR_CUDA,
                     std::string("workspace allocation: ") + cudaGetErrorString(e));
     }
-    e = cudaMemcpy(ws->desc.as<char>(np.tasks_off), np.tasks.data(), sizeof(FusedTask) * T, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !np.segs.empty())
-        e = cudaMemcpy(ws->desc.as<char>(np.segs_off), np.segs.data(), sizeof(FusedSeg) * np.segs.size(),
-                       cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !np.jobs.empty())
-        e = cudaMemcpy(ws->desc.as<char>(np.jobs_off), np.jobs.data(), sizeof(SampleJob) * np.jobs.size(),
-                       cudaMemcpyHostToDevice);
-    if (e == cudaSuccess && !np.merge_tasks.empty())
-        e = cudaMemcpy(ws->desc.as<char>(np.merge_off), np.merge_tasks.data(), sizeof(int32_t) * np.merge_tasks.size(),
-                       cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, L.bytes);
+    if (use_upload) {
+        // Stage the whole descriptor block in pinned memory, one async copy.
+        if (ws->h_stage_bytes < desc_bytes) {
+            if (ws->h_stage) cudaFreeHost(ws->h_stage);
+            ws->h_stage = nullptr;
+            ws->h_stage_bytes = 0;
+            e = cudaMallocHost(&ws->h_stage, desc_bytes);
+            if (e == cudaSuccess) ws->h_stage_bytes = desc_bytes;
+        }
+        if (e == cudaSuccess) {
+            if (T) std::memcpy(ws->h_stage + np.tasks_off, np.tasks.data(), sizeof(FusedTask) * T);
+            if (!np.segs.empty())
+                std::memcpy(ws->h_stage + np.segs_off, np.segs.data(), sizeof(FusedSeg) * np.segs.size());
+            if (!np.jobs.empty())
+                std::memcpy(ws->h_stage + np.jobs_off, np.jobs.data(), sizeof(SampleJob) * np.jobs.size());
+            if (!np.merge_tasks.empty())
+                std::memcpy(ws->h_stage + np.merge_off, np.merge_tasks.data(),
+                            sizeof(int32_t) * np.merge_tasks.size());
+            e = cudaMemcpyAsync(ws->desc.p, ws->h_stage, desc_bytes, cudaMemcpyHostToDevice, upload);
+        }
+        if (e == cudaSuccess) e = cudaMemsetAsync(ws->state.p, 0, L.bytes, upload);
+    } else {
+        e = cudaMemcpy(ws->desc.as<char>(np.tasks_off), np.tasks.data(), sizeof(FusedTask) * T, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !np.segs.empty())
+            e = cudaMemcpy(ws->desc.as<char>(np.segs_off), np.segs.data(), sizeof(FusedSeg) * np.segs.size(),
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !np.jobs.empty())
+            e = cudaMemcpy(ws->desc.as<char>(np.jobs_off), np.jobs.data(), sizeof(SampleJob) * np.jobs.size(),
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !np.merge_tasks.empty())
+            e = cudaMemcpy(ws->desc.as<char>(np.merge_off), np.merge_tasks.data(),
+                           sizeof(int32_t) * np.merge_tasks.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, L.bytes);
+    }
     if (e == cudaSuccess && np.fused && !np.jobs.empty()) {
         SampleKernel sk = pick_sample(scale);
         const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
@@ -764,6 +793,7 @@ int radik_ws_destroy(radik_ws* ws) {
                       &ws->stage, &ws->pcand[0], &ws->pcand[1], &ws->io_in, &ws->io_idx, &ws->io_vout, &ws->io_iout})
         b->release();
     if (ws->h_err) cudaFreeHost(ws->h_err);
+    if (ws->h_stage) cudaFreeHost(ws->h_stage);
     delete ws;
     return RADIK_OK;
 }
@@ -1192,3 +1222,5 @@ int radik_filter(float* d_val_out, void* d_idx_out, int idx_bytes, int32_t* d_co
 }
 
 }  // extern "C"
+
+#include "server.inl"
