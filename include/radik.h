@@ -87,6 +87,18 @@ typedef struct radik_plan_info {
  * RADIK_ERR_INVALID when the workspace has no plan yet. */
 int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info);
 
+/* Autotuner (engine-specific, no reference counterpart): runs the call
+ * below on the caller's data with each candidate configuration of the fused
+ * path (kernel form, block and ring shape, sample size, segment size),
+ * `reps` timed calls each, and keeps the fastest in ws for this batch shape
+ * (task_lens, k, flags, index width); later calls with that shape use it.
+ * The outputs hold a valid result afterwards.  *chosen (nullable) describes
+ * the chosen plan, *best_ms (nullable) its time per call.  Not during
+ * stream capture. */
+int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_val_in,
+                      const void* d_idx_in, const int64_t* h_task_lens, int64_t num_tasks, int64_t k,
+                      uint32_t flags, void* stream, int reps, radik_plan_info* chosen, double* best_ms);
+
 /* topk_radix_select!(val_out, idx_out, ws, val_in, idx_in, task_lens, k,
  *                    Val(LARGEST), Val(ASCEND), Val(WITHSCALE), Val(WITHIDXIN),
  *                    Val(WITHPACKING), Val(VLOAD_SIZE_BYTES))

@@ -134,6 +134,28 @@ class RadiKWorkspace:
         check(load().radik_ws_plan_info(self._h, ctypes.byref(info)))
         return {n: getattr(info, n) for n, _ in PlanInfo._fields_}
 
+    def autotune(self, val_out, idx_out, val_in, idx_in, task_lens, k: int, largest: bool = True,
+                 ascend: bool = True, withscale: bool = False, withidxin: bool = False, *, reps: int = 5,
+                 stream=None) -> dict:
+        """Time the fused path's candidate configurations on this batch and
+        keep the fastest for its shape (radik_ws_autotune); returns the chosen
+        plan with its time per call ("ms")."""
+        from ._lib import PlanInfo
+        _check_cuda(val_out, "val_out")
+        _check_cuda(idx_out, "idx_out")
+        _check_cuda(val_in, "val_in")
+        lens = _lens_array(task_lens)
+        info = PlanInfo()
+        ms = ctypes.c_double()
+        flags = _flags(largest, ascend, withscale, withidxin)
+        check(load().radik_ws_autotune(self._h, _ptr(val_out), _ptr(idx_out), _idx_bytes(idx_out.dtype), _ptr(val_in),
+                                       _ptr(idx_in) if withidxin else None, lens.ctypes.data_as(ctypes.c_void_p),
+                                       len(lens), int(k), flags, _stream(stream), int(reps), ctypes.byref(info),
+                                       ctypes.byref(ms)))
+        out = {n: getattr(info, n) for n, _ in PlanInfo._fields_}
+        out["ms"] = ms.value
+        return out
+
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             load().radik_ws_destroy(self._h)

@@ -29,7 +29,7 @@ STATUS = {
 # Every symbol include/radik.h declares (checked by the CPU test suite).
 EXPORTS = (
     "radik_ws_create", "radik_ws_destroy", "radik_ws_bytes", "radik_ws_error", "radik_ws_prepare",
-    "radik_ws_plan_info",
+    "radik_ws_plan_info", "radik_ws_autotune",
     "radik_topk_radix_select", "radik_topk", "radik_topk_host", "radik_topk_noalloc",
     "radik_count_bin_ex", "radik_count_bin", "radik_select_bin", "radik_filter",
     "radik_last_error", "radik_status_string", "radik_version",
@@ -80,6 +80,8 @@ def _declare(L: ctypes.CDLL) -> None:
     L.radik_ws_error.argtypes = [P, ctypes.POINTER(U32)]
     L.radik_ws_prepare.argtypes = [P, P, I64, I64, U32, I]
     L.radik_ws_plan_info.argtypes = [P, ctypes.POINTER(PlanInfo)]
+    L.radik_ws_autotune.argtypes = [P, P, P, I, P, P, P, I64, I64, U32, P, I, ctypes.POINTER(PlanInfo),
+                                    ctypes.POINTER(ctypes.c_double)]
     L.radik_topk_radix_select.argtypes = [P, P, I, P, P, P, P, I64, I64, U32, P]
     L.radik_topk.argtypes = [P, P, I, P, I64, P, I64, P, I64, I64, I, I, P]
     L.radik_topk_host.argtypes = [P, P, I, P, I64, P, I64, P, I64, I64, I, I, P, P]

@@ -138,6 +138,36 @@ int env_int(const char* name, int dflt) {
     return (v && *v) ? std::atoi(v) : dflt;
 }
 
+// Tunable shape of a plan.  Defaults are the measured best for the common
+// cases; radik_ws_autotune picks another per batch shape; environment
+// variables (RADIK_WS, RADIK_WST, RADIK_WSJ, RADIK_WSS, RADIK_WS_SAMPLE,
+// RADIK_WS_WINDOWS, RADIK_SEG_DIV) override both, for experiments.
+struct TuneConfig {
+    int form = -1;          // -1 automatic, 0 barrier form, 1 warp-specialised form
+    int ws_threads = 128;   // warp-specialised: consumer threads
+    int ws_j = 8;           // float4 per lane in a warp tile
+    int ws_stages = 8;      // ring stages (a multiple of the consumer warps)
+    int sample_max = 2048;  // single-segment sample (elements)
+    int sample_windows = 2; // digit windows of its rank threshold
+    int seg_div = 3;        // work items per resident block when splitting tasks
+    bool operator==(const TuneConfig& o) const {
+        return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
+               sample_max == o.sample_max && sample_windows == o.sample_windows && seg_div == o.seg_div;
+    }
+};
+
+TuneConfig with_env(TuneConfig c) {
+    c.form = env_int("RADIK_WS", c.form);
+    c.ws_threads = env_int("RADIK_WST", c.ws_threads);
+    c.ws_j = env_int("RADIK_WSJ", c.ws_j);
+    c.ws_stages = env_int("RADIK_WSS", c.ws_stages);
+    c.sample_max = env_int("RADIK_WS_SAMPLE", c.sample_max);
+    c.sample_windows = env_int("RADIK_WS_WINDOWS", c.sample_windows);
+    c.seg_div = std::max(1, env_int("RADIK_SEG_DIV", c.seg_div));
+    if (c.sample_max != 2048 && c.sample_max != 4096) c.sample_max = 2048;
+    return c;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -148,8 +178,9 @@ struct PlanKey {
     int64_t k = -1;
     uint32_t flags = 0;
     int idx_bytes = 0;
+    TuneConfig tune;
     bool operator==(const PlanKey& o) const {
-        return k == o.k && flags == o.flags && idx_bytes == o.idx_bytes && lens == o.lens;
+        return k == o.k && flags == o.flags && idx_bytes == o.idx_bytes && lens == o.lens && tune == o.tune;
     }
 };
 
@@ -202,6 +233,8 @@ struct radik_ws {
     DevBuf pcand[2];  // plain: [N] each
     DevBuf io_in, io_idx, io_vout, io_iout;  // host-buffer entry point
     Plan plan;
+    // Configurations chosen by radik_ws_autotune, by batch shape.
+    std::vector<std::pair<PlanKey, TuneConfig>> tuned;
 };
 
 namespace {
@@ -246,10 +279,10 @@ size_t fused_cap(size_t k, size_t tile, int threads) {
 
 // Segment length: about three work items per resident block, at least 64
 // tiles, a multiple of the tile (env RADIK_SEG overrides).
-int64_t pick_seg_len(int64_t N, int64_t resident, size_t tile, bool fused) {
+int64_t pick_seg_len(int64_t N, int64_t resident, size_t tile, bool fused, int seg_div) {
     int64_t seg_len = env_int("RADIK_SEG", 0);
     if (seg_len <= 0) {
-        const int64_t target = N / std::max<int64_t>(1, 3 * resident);
+        const int64_t target = N / std::max<int64_t>(1, seg_div * resident);
         seg_len = std::max<int64_t>(64 * static_cast<int64_t>(tile), target);
     }
     seg_len = static_cast<int64_t>(round_up(static_cast<size_t>(seg_len), tile));
@@ -350,7 +383,7 @@ int set_smem_and_occupancy(const void* fn, int threads, size_t smem) {
 
 // Host half of a launch plan: kernel configuration, segment table, sample
 // jobs and descriptor offsets.  Allocates no device memory.
-int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& np) {
+int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& np, const TuneConfig& tc) {
     const DeviceInfo di = device_info();
     np.T = T;
     np.N = 0;
@@ -365,18 +398,17 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     // warp tiles of 128 * RADIK_WSJ elements, RADIK_WSS ring stages.
     const int bar_threads = env_int("RADIK_THREADS", 256);
     const int bar_vec = env_int("RADIK_VEC", 8);
-    const int ws_env = env_int("RADIK_WS", -1);
-    const int ws_j = env_int("RADIK_WSJ", 8);
-    const int ws_threads = env_int("RADIK_WST", 128);
-    np.ws_stages = env_int("RADIK_WSS", 8);
-    np.ws_sample_max = env_int("RADIK_WS_SAMPLE", 2048);
-    np.ws_sample_windows = env_int("RADIK_WS_WINDOWS", 2);
-    if (np.ws_sample_max != 2048 && np.ws_sample_max != 4096) np.ws_sample_max = 2048;
+    const int ws_env = tc.form;
+    const int ws_j = tc.ws_j;
+    const int ws_threads = tc.ws_threads;
+    np.ws_stages = tc.ws_stages;
+    np.ws_sample_max = tc.sample_max;
+    np.ws_sample_windows = tc.sample_windows;
     const size_t seg_tile = 2048;  // segments are whole tiles of either form
 
     // Segments and samples first, sized for the warp-specialised form's
     // residency (four blocks per SM).
-    segment_tasks(np, lens, T, k, flags, pick_seg_len(np.N, 4LL * di.sms, seg_tile, !plain), !plain);
+    segment_tasks(np, lens, T, k, flags, pick_seg_len(np.N, 4LL * di.sms, seg_tile, !plain, tc.seg_div), !plain);
     bool all_flush = T > 0;  // every non-empty task is split and sampled
     for (int64_t t = 0; t < T; ++t)
         if (lens[t] > 0 && (np.tasks[t].flags & kTaskSampled) == 0) all_flush = false;
@@ -429,8 +461,8 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     if (!np.fused || !np.ws_form) {
         // Re-segment for the form that runs.
         occ = std::max(occ, 1);
-        segment_tasks(np, lens, T, k, flags, pick_seg_len(np.N, static_cast<int64_t>(occ) * di.sms, seg_tile, np.fused),
-                      np.fused);
+        segment_tasks(np, lens, T, k, flags,
+                      pick_seg_len(np.N, static_cast<int64_t>(occ) * di.sms, seg_tile, np.fused, tc.seg_div), np.fused);
     }
     const int64_t resident = static_cast<int64_t>(occ) * di.sms;
     np.merge_tasks.clear();
@@ -466,22 +498,42 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
 size_t plan_desc_bytes(const Plan& pl) { return pl.merge_off + sizeof(int32_t) * pl.merge_tasks.size(); }
 
 // Build the launch plan for a batch shape and size the workspace for it.
+// Key of a call's plan: the batch shape and the configuration that applies
+// to it (one chosen by radik_ws_autotune for this shape, else the defaults),
+// with environment overrides on top.
+PlanKey plan_key(const radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes,
+                 const TuneConfig* force = nullptr) {
+    PlanKey key;
+    key.lens.assign(lens, lens + T);
+    key.k = k;
+    key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
+    key.idx_bytes = idx_bytes;
+    TuneConfig tc;
+    if (force) {
+        tc = *force;
+    } else {
+        for (const auto& e : ws->tuned) {
+            PlanKey kk = key;
+            kk.tune = e.first.tune;
+            if (e.first == kk) { tc = e.second; break; }
+        }
+    }
+    key.tune = with_env(tc);
+    return key;
+}
+
 // With `upload` set, descriptors are uploaded with copies ordered on that
 // stream from pinned staging memory (the request server: no host wait, no
 // legacy-stream synchronisation); otherwise synchronously.
 int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes,
                cudaStream_t upload = nullptr, bool use_upload = false) {
     Plan& pl = ws->plan;
-    PlanKey key;
-    key.lens.assign(lens, lens + T);
-    key.k = k;
-    key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
-    key.idx_bytes = idx_bytes;
+    PlanKey key = plan_key(ws, lens, T, k, flags, idx_bytes);
     if (pl.valid && pl.key == key) return RADIK_OK;
 
     Plan np;
     np.key = key;
-    int rc = plan_shape(lens, T, k, flags, np);
+    int rc = plan_shape(lens, T, k, flags, np, key.tune);
     if (rc) return rc;
     const bool scale = (flags & RADIK_WITHSCALE) != 0;
     const size_t kk = static_cast<size_t>(k);
@@ -875,11 +927,7 @@ int radik_topk_radix_select(float* d_val_out, void* d_idx_out, int idx_bytes, ra
         ((flags & RADIK_WITHIDXIN) && (reinterpret_cast<uintptr_t>(d_idx_in) & (idx_bytes - 1))))
         return fail(RADIK_ERR_INVALID, "device arrays must be aligned to their element size");
     {
-        PlanKey key;
-        key.lens.assign(h_task_lens, h_task_lens + num_tasks);
-        key.k = k;
-        key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
-        key.idx_bytes = idx_bytes;
+        const PlanKey key = plan_key(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
         if (!(ws->plan.valid && ws->plan.key == key)) {
             if (cap != cudaStreamCaptureStatusNone)
                 return fail(RADIK_ERR_CAPTURE, "no prepared plan for this shape: call radik_ws_prepare before capture");
@@ -898,6 +946,76 @@ int radik_topk_radix_select(float* d_val_out, void* d_idx_out, int idx_bytes, ra
     if (rc) return rc;
     if (flags & RADIK_ASYNC) return RADIK_OK;
     return finish_sync(ws, s);
+}
+
+int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_val_in,
+                      const void* d_idx_in, const int64_t* h_task_lens, int64_t num_tasks, int64_t k, uint32_t flags,
+                      void* stream, int reps, radik_plan_info* chosen, double* best_ms) {
+    if (!ws || !h_task_lens) return fail(RADIK_ERR_INVALID, "NULL argument");
+    if (num_tasks <= 0 || k <= 0) return fail(RADIK_ERR_INVALID, "num_tasks and k must be positive");
+    if (flags & RADIK_PLAIN) return fail(RADIK_ERR_INVALID, "the multi-pass path has nothing to tune");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus capst = cudaStreamCaptureStatusNone;
+    RADIK_CUDA(cudaStreamIsCapturing(s, &capst));
+    if (capst != cudaStreamCaptureStatusNone) return fail(RADIK_ERR_CAPTURE, "autotuning cannot run during capture");
+    reps = std::max(1, std::min(reps, 100));
+    // Candidate shapes: the defaults, other rings and block sizes of the
+    // warp-specialised form, a larger sample, the barrier form, and other
+    // segment sizes for split tasks.
+    std::vector<TuneConfig> cands;
+    TuneConfig d;
+    cands.push_back(d);
+    { TuneConfig c = d; c.form = 1; c.ws_stages = 12; cands.push_back(c); }
+    { TuneConfig c = d; c.form = 1; c.ws_threads = 256; c.ws_stages = 16; cands.push_back(c); }
+    { TuneConfig c = d; c.form = 1; c.sample_max = 4096; cands.push_back(c); }
+    { TuneConfig c = d; c.form = 0; cands.push_back(c); }
+    { TuneConfig c = d; c.seg_div = 2; cands.push_back(c); }
+    { TuneConfig c = d; c.seg_div = 6; cands.push_back(c); }
+    PlanKey base = plan_key(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
+    auto set_choice = [&](const TuneConfig& c) {
+        for (auto& e : ws->tuned) {
+            PlanKey kk = base;
+            kk.tune = e.first.tune;
+            if (e.first == kk) { e.second = c; return; }
+        }
+        ws->tuned.emplace_back(base, c);
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RADIK_CUDA(cudaEventCreate(&e0));
+    RADIK_CUDA(cudaEventCreate(&e1));
+    double best = 1e30;
+    TuneConfig best_c = d;
+    int rc = RADIK_OK;
+    for (const TuneConfig& c : cands) {
+        set_choice(c);
+        const uint32_t af = flags | RADIK_ASYNC;
+        rc = radik_topk_radix_select(d_val_out, d_idx_out, idx_bytes, ws, d_val_in, d_idx_in, h_task_lens, num_tasks,
+                                     k, af, stream);  // builds the plan, warms up
+        if (rc == RADIK_OK) rc = finish_sync(ws, s);
+        if (rc != RADIK_OK) continue;  // this shape does not apply here
+        cudaEventRecord(e0, s);
+        for (int i = 0; i < reps && rc == RADIK_OK; ++i)
+            rc = radik_topk_radix_select(d_val_out, d_idx_out, idx_bytes, ws, d_val_in, d_idx_in, h_task_lens,
+                                         num_tasks, k, af, stream);
+        cudaEventRecord(e1, s);
+        if (rc == RADIK_OK) rc = finish_sync(ws, s);
+        if (rc != RADIK_OK) continue;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms / reps < best) {
+            best = ms / reps;
+            best_c = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best >= 1e30) return rc != RADIK_OK ? rc : fail(RADIK_ERR_INVALID, "no configuration ran");
+    set_choice(best_c);
+    rc = build_plan(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
+    if (rc) return rc;
+    if (chosen) radik_ws_plan_info(ws, chosen);
+    if (best_ms) *best_ms = best;
+    return RADIK_OK;
 }
 
 int radik_topk(float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_data, int64_t data_len,
@@ -1060,7 +1178,7 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
     view.n = maxlen;
     view.num_tasks = num_tasks;
     view.index_bytes = idx_bytes;
-    rc = plan_shape(h_task_lens, num_tasks, k, flags, view.plan);
+    rc = plan_shape(h_task_lens, num_tasks, k, flags, view.plan, with_env(TuneConfig{}));
     if (rc) return rc;
     const Plan& pl = view.plan;
     if (!pl.fused) return fail(RADIK_ERR_WS_TOO_SMALL, "the fused kernel's candidate buffer does not fit for this k");

@@ -148,3 +148,28 @@ def test_host_buffer_entry_point(radik, torch_cuda, oracle):
     v, i = radik.topk_host(x, lens, 77, largest=False, rev=True)
     ov, oi = oracle.topk(x, lens, 77, largest=False, rev=True)
     assert np.array_equal(v, ov) and np.array_equal(i, oi)
+
+
+def test_autotune_keeps_results_exact(oracle, radik, torch_cuda):
+    """radik_ws_autotune times the candidate configurations on the batch and
+    keeps the fastest for its shape; results stay identical to the oracle
+    under the chosen configuration and on later calls."""
+    torch = torch_cuda
+    rng = np.random.default_rng(99)
+    lens = [40_000] * 24 + [300_000, 7]
+    k = 128
+    h = rng.standard_normal(sum(lens)).astype(np.float32)
+    x = torch.from_numpy(h).cuda()
+    vo = torch.empty((len(lens), k), device="cuda")
+    io = torch.empty((len(lens), k), dtype=torch.int32, device="cuda")
+    ws = radik.RadiKWorkspace("cuda", max(lens), len(lens))
+    info = ws.autotune(vo, io, x, None, lens, k, True, True, reps=2)
+    assert info["ms"] > 0 and info["path"] in (0, 1) and info["grid"] > 0
+    ov, oi = oracle.topk(h, lens, k)
+    for _ in range(2):
+        vo.fill_(7.0)
+        radik.topk_radix_select_(vo, io, ws, x, None, lens, k, True, True)
+        assert np.array_equal(vo.cpu().numpy().view(np.uint32), ov.view(np.uint32))
+        assert np.array_equal(io.cpu().numpy().astype(np.int64), oi.astype(np.int64))
+        assert ws.plan_info()["path"] == info["path"]
+    ws.close()
