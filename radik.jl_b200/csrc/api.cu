@@ -126,6 +126,8 @@ constexpr int kMergeThreads = 1024;  // one block per flush-mode task
 MergeKernel pick_merge(bool scale) {
     return scale ? merge_topk_kernel<kMergeThreads, true> : merge_topk_kernel<kMergeThreads, false>;
 }
+MergeKernel pick_rank(bool scale) { return scale ? rank_write_kernel<true> : rank_write_kernel<false>; }
+constexpr size_t kRankSmem = sizeof(uint64_t) * (kRankMaxK + 2);
 
 using SampleKernel = void (*)(FusedParams, const SampleJob*, uint64_t*, uint32_t*);
 
@@ -244,7 +246,7 @@ namespace {
 struct StateLayout {
     // kAny: multi-pass path: some task still active; fused path: some task failed.
     static constexpr size_t kErr = 0, kWork = 4, kWorkRetry = 8, kAny = 12, kHeader = 16;
-    size_t gthr, gthr_r, done, done_r, cnt, cnt_r, fail, sdone, bytes;
+    size_t gthr, gthr_r, done, done_r, cnt, cnt_r, fail, sdone, rk, bytes;
     explicit StateLayout(int64_t T) {
         const size_t t8 = round_up(sizeof(uint64_t) * static_cast<size_t>(std::max<int64_t>(T, 1)), 16);
         const size_t t4 = round_up(sizeof(uint32_t) * static_cast<size_t>(std::max<int64_t>(T, 1)), 16);
@@ -256,7 +258,8 @@ struct StateLayout {
         cnt_r = cnt + t4;
         fail = cnt_r + t4;
         sdone = fail + t4;
-        bytes = sdone + t4;
+        rk = sdone + t4;
+        bytes = rk + t4;
     }
 };
 
@@ -484,8 +487,10 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
         np.retry_threads = bar_threads;
         np.retry_vec = bar_vec;
     }
-    if (np.fused && !np.merge_tasks.empty())
+    if (np.fused && !np.merge_tasks.empty()) {
         set_smem_and_occupancy(reinterpret_cast<const void*>(pick_merge(scale)), kMergeThreads, np.merge_smem);
+        set_smem_and_occupancy(reinterpret_cast<const void*>(pick_rank(scale)), kRankThreads, kRankSmem);
+    }
     np.tasks_off = 0;
     np.segs_off = round_up(sizeof(FusedTask) * T, 256);
     np.jobs_off = np.segs_off + round_up(sizeof(FusedSeg) * np.segs.size(), 256);
@@ -642,6 +647,7 @@ FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, c
     p.sample_windows = static_cast<uint32_t>(pl.ws_sample_windows);
     p.cand = ws->cand.as<uint64_t>();
     p.sort_scratch = ws->scratch.as<uint64_t>();
+    p.rank_ready = ws->state.as<uint32_t>(L.rk);
     return p;
 }
 
@@ -668,6 +674,12 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
         m.cap = pl.merge_cap;
         pick_merge(scale)<<<static_cast<unsigned>(pl.merge_tasks.size()), kMergeThreads, pl.merge_smem, s>>>(
             m, ws->desc.as<int32_t>(pl.merge_off));
+        RADIK_CUDA(cudaGetLastError());
+        // ... and the output rows of those it left to the rank kernel.
+        const dim3 rgrid(static_cast<unsigned>((p.kmax + kRankPerBlock - 1) / kRankPerBlock),
+                         static_cast<unsigned>(pl.merge_tasks.size()));
+        const size_t rsmem = sizeof(uint64_t) * (std::min<size_t>(p.kmax, kRankMaxK) + 2);
+        pick_rank(scale)<<<rgrid, kRankThreads, rsmem, s>>>(m, ws->desc.as<int32_t>(pl.merge_off));
         RADIK_CUDA(cudaGetLastError());
     }
     if (!pl.jobs.empty()) {
@@ -885,7 +897,7 @@ int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
     // fused: sampling kernel + fused kernel (+ merge kernel for flush-mode
     // tasks) + retry launch when sampled;
     // multi-pass: histogram, select, compact, advance, finalize at least.
-    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 1) : 5;
+    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) : 5;
     return RADIK_OK;
 }
 

@@ -89,6 +89,7 @@ struct FusedParams {
     uint32_t* work_counter;  // [1]
     uint64_t* cand;          // candidate regions
     uint64_t* sort_scratch;  // [gridDim.x * kmax] (kmax > 4096 only)
+    uint32_t* rank_ready;    // [T] merge kernel left the k output keys for rank_write_kernel (nullable)
     uint32_t* err;
 };
 

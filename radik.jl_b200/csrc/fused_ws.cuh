@@ -151,6 +151,7 @@ __device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, u
     constexpr uint32_t TW = 128u * J;  // elements per warp tile
     constexpr uint32_t kChunksPerTile = TW / kSampleChunkLen;
     static_assert((kSampleMax / 2) % TW == 0 && TW % kSampleChunkLen == 0, "sample tiles");
+    const uint64_t pol = l2_evict_first_policy();  // the input is read once
     uint32_t g = 0;            // tiles issued
     uint32_t st = 0, eph = 1;  // stage of tile g; parity of the "empty" phase it must wait for
     for (uint32_t d = 0;; ++d) {
@@ -179,13 +180,14 @@ __device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, u
             if (i < ns) {
                 mbar_arrive_expect_tx(full + st, TW * 4u);
                 for (uint32_t c = 0; c < kChunksPerTile; ++c)
-                    bulk_load(dst + c * kSampleChunkLen, tv.data + ws_sample_pos(tv.len, mis, i * kChunksPerTile + c, nch),
-                              kSampleChunkLen * 4u, full + st);
+                    bulk_load_hint(dst + c * kSampleChunkLen,
+                                   tv.data + ws_sample_pos(tv.len, mis, i * kChunksPerTile + c, nch), kSampleChunkLen * 4u,
+                                   full + st, pol);
             } else {
                 const int64_t e0 = static_cast<int64_t>(i - ns) * TW;
                 const uint32_t bytes = static_cast<uint32_t>(min(static_cast<int64_t>(TW), G.nvec * 4 - e0)) * 4u;
                 mbar_arrive_expect_tx(full + st, bytes);
-                bulk_load(dst, tv.data + G.a0 + e0, bytes, full + st);
+                bulk_load_hint(dst, tv.data + G.a0 + e0, bytes, full + st, pol);
             }
             if (++st == static_cast<uint32_t>(STAGES)) { st = 0; eph ^= 1u; }
         }

@@ -2,38 +2,234 @@
 //
 // In flush mode (fused_ws.cuh) every segment of a large sampled task wrote
 // all its elements above the task's seeded threshold to the task's candidate
-// region: a superset of the task's k best.  One block per such task loads the
-// region into shared memory (all of it when it fits, which the host sizes for;
-// otherwise in chunks, keeping a few more than k with block_shrink whenever
-// the buffer fills), selects the exact k best, sorts them and writes the
-// task's row.  If fewer than k candidates exist (the sampled threshold was
-// above the task's k-th composite) or the region overflowed, the task is
-// flagged and the retry launch recomputes it without the sample.
+// region: a superset of the task's k best.  One block per such task selects
+// the exact k best of the region:
+//   * usual case (the region fits in shared memory beside the scratch below,
+//     k <= kRankMaxK): the region is loaded at once and the k-th largest
+//     composite is found with 8-bit digit windows (per-warp histograms) that
+//     narrow it to one bin, whose entries one warp then bisects; the k
+//     selected entries are written back to the region as output sort keys,
+//     and rank_write_kernel
+//     puts every one at its place in the output row: its place is the number
+//     of the k keys below it, counted by many blocks at once (k^2 compares
+//     spread over the GPU instead of a sorting network on one SM);
+//   * otherwise the region is loaded into shared memory (in chunks, keeping a
+//     few more than k with block_shrink whenever the buffer fills), selected
+//     with block_select_topk, sorted and written by this block.
+// If fewer than k candidates exist (the sampled threshold was above the
+// task's k-th composite) or the region overflowed, the task is flagged and
+// the retry launch recomputes it without the sample.
 #pragma once
 
 #include "fused.cuh"
 
 namespace radik {
 
+constexpr uint32_t kRankMaxK = 8192;   // largest k whose row rank_write_kernel writes
+constexpr int kRankThreads = 256;      // rank_write_kernel: threads per block
+constexpr int kRankSplit = 16;         // threads counting for one output key
+constexpr int kRankPerBlock = kRankThreads / kRankSplit;  // output keys placed per block
+
+constexpr uint32_t kWarpBisect = 512;  // boundary-bin entries one warp finishes (16 per lane)
+
+// Bound of the k best among buf[0, n) (unique composites in shared memory,
+// 1 <= k <= n; vor and vand span them).  8-bit digit windows below the
+// common prefix narrow the entries in play to the bin holding rank k: every
+// warp counts into its own histogram (whist, 256 words per warp: no
+// contention between warps on the few bins that most entries fall into), the
+// histograms are summed and searched for rank k.  Once that bin holds at
+// most kWarpBisect entries they are copied to `spill` and warp 0 finds the
+// exact bound by bisection over their bits.  Returns tau with exactly k
+// entries >= tau.  All threads call.
+template <int THREADS>
+__device__ uint64_t block_topk_bound(const uint64_t* buf, uint32_t n, uint32_t k, uint64_t vor, uint64_t vand,
+                                     BlockScratch<THREADS>& s, uint32_t* whist, uint64_t* spill, uint32_t* spill_n,
+                                     unsigned long long* result, uint32_t* err) {
+    constexpr int W = 8;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u;
+    const uint64_t diff = vor ^ vand;
+    if (diff == 0ull) return vand;  // a single entry
+    int top = 63 - __clzll(static_cast<long long>(diff));
+    uint64_t prefix = (top >= 63) ? 0ull : (vand >> (top + 1));
+    int pbits = 63 - top;  // bits above `top` shared by the entries still in play
+    uint32_t r = k;
+    for (int guard = 0; guard < 9; ++guard) {
+        const int w = top + 1 < W ? top + 1 : W;
+        const int sh = top + 1 - w;
+        const uint32_t nb = 1u << w;
+        uint32_t* my = whist + (tid >> 5) * 256u;
+        for (uint32_t i = lane; i < nb; i += 32) my[i] = 0;
+        __syncwarp();
+        for (uint32_t i = tid; i < n; i += THREADS) {
+            const uint64_t c = buf[i];
+            if (pbits == 0 || (c >> (sh + w)) == prefix) atomicAdd(my + (static_cast<uint32_t>(c >> sh) & (nb - 1)), 1u);
+        }
+        block_sync<THREADS>();
+        for (uint32_t i = tid; i < nb; i += THREADS) {
+            uint32_t sum = 0;
+#pragma unroll 8
+            for (int ww = 0; ww < THREADS / 32; ++ww) sum += whist[ww * 256 + i];
+            s.hist[i] = sum;
+        }
+        block_sync<THREADS>();
+        block_rank_search<THREADS>(r, nb, s);
+        const uint32_t b = s.bc32[0], rr = s.bc32[1], cb = s.bc32[2];
+        block_sync<THREADS>();  // hist and bc32 are rewritten by the next window
+        if (cb == 0xffffffffu) {  // never expected: rank k lies beyond the entries
+            if (tid == 0) record_error(err, kErrInternal);
+            return vand;
+        }
+        const uint64_t bin_prefix = (pbits == 0) ? b : ((prefix << w) | b);
+        if (cb == rr || sh == 0) return bin_prefix << sh;  // the whole bin is in: k entries >= its lower edge
+        if (cb <= kWarpBisect) {
+            // The boundary bin to `spill`; warp 0 finds its rr-th largest.
+            if (tid == 0) *spill_n = 0;
+            block_sync<THREADS>();
+            const uint32_t lt = lanemask_lt();
+            for (uint32_t base = 0; base < n; base += THREADS) {
+                const uint32_t i = base + tid;
+                const uint64_t c = i < n ? buf[i] : 0ull;
+                const bool in = i < n && (c >> sh) == bin_prefix;
+                const uint32_t m = __ballot_sync(kFullMask, in);
+                if (m == 0u) continue;
+                const uint32_t leader = __ffs(m) - 1;
+                uint32_t o = 0;
+                if (lane == leader) o = atomicAdd(spill_n, __popc(m));
+                o = __shfl_sync(kFullMask, o, leader);
+                if (in && o + __popc(m & lt) < kWarpBisect) spill[o + __popc(m & lt)] = c;
+            }
+            block_sync<THREADS>();
+            if (tid < 32) {
+                const uint32_t cnt = *spill_n < kWarpBisect ? *spill_n : kWarpBisect;
+                uint64_t wor = 0, wand = ~0ull;
+                for (uint32_t i = lane; i < cnt; i += 32) {
+                    wor |= spill[i];
+                    wand &= spill[i];
+                }
+#pragma unroll
+                for (int m = 16; m > 0; m >>= 1) {
+                    wor |= __shfl_xor_sync(kFullMask, wor, m);
+                    wand &= __shfl_xor_sync(kFullMask, wand, m);
+                }
+                uint64_t tau = wand;
+                const uint64_t d = wor ^ wand;
+                if (d != 0ull && rr <= cnt) {
+                    int bb = 63 - __clzll(static_cast<long long>(d));
+                    tau = (bb == 63) ? 0ull : (wand & ~((2ull << bb) - 1));
+                    uint32_t cge = cnt;
+                    for (; bb >= 0 && cge != rr; --bb) {
+                        const uint64_t cand = tau | (1ull << bb);
+                        uint32_t c = 0;
+                        for (uint32_t i = lane; i < cnt; i += 32) c += (spill[i] >= cand) ? 1u : 0u;
+                        c = __reduce_add_sync(kFullMask, c);
+                        if (c >= rr) {
+                            tau = cand;
+                            cge = c;
+                        }
+                    }
+                }
+                if (lane == 0) {
+                    if (cnt != cb) record_error(err, kErrInternal);
+                    *result = tau;
+                }
+            }
+            block_sync<THREADS>();
+            return *result;
+        }
+        prefix = bin_prefix;
+        pbits += w;
+        r = rr;
+        top = sh - 1;
+    }
+    if (tid == 0) record_error(err, kErrInternal);
+    return prefix;
+}
+
 template <int THREADS, bool kScale>
 __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, const int32_t* merge_tasks) {
     extern __shared__ __align__(16) uint64_t s_buf[];
     __shared__ FusedShared<THREADS> sh;
+    __shared__ uint32_t s_spill_n;        // block_topk_bound_regs: entries of the boundary bin
+    __shared__ unsigned long long s_tau;  // ... and the bound warp 0 found
     const int tid = threadIdx.x;
     const int t = merge_tasks[blockIdx.x];
-    if (*reinterpret_cast<volatile const uint32_t*>(p.fail + t) != 0u) return;  // the retry launch redoes it
+    // The task's flag, descriptor and candidate count, loaded together.
+    const uint32_t failed = __ldcg(p.fail + t);
     const FusedTask td = p.tasks[t];
+    const uint32_t have = __ldcg(p.task_cnt + t);
+    if (failed != 0u) return;  // the retry launch redoes it
     const TaskView tv = task_view<kScale>(p, t, td);
     const uint32_t k = tv.k;
     const uint32_t cap = p.cap;
     const uint32_t region = static_cast<uint32_t>(td.nseg) * p.kmax;
-    const uint32_t have = *reinterpret_cast<volatile const uint32_t*>(p.task_cnt + t);
     const uint32_t n = have < region ? have : region;
     const unsigned long long* src = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
     // Room kept free while streaming chunks: a shrink keeps at most mid_keep.
     const uint32_t mid_keep = k + (cap - k) / 4;
     if (tid == 0) sh.cnt = 0;
     block_sync<THREADS>();
+    // Shared memory of the usual case: the region, then per-warp histograms
+    // (256 words per warp), then the boundary bin.
+    const uint32_t hist_off = (n + 1) & ~1u;
+    const uint32_t spill_off = hist_off + (THREADS / 32) * 256 / 2;
+    if (p.rank_ready != nullptr && spill_off + kWarpBisect <= cap && hist_off + k <= cap && k <= kRankMaxK &&
+        k <= region) {
+        if (n < k) {  // fewer than k candidates: the sampled threshold was too high
+            if (tid == 0) {
+                p.fail[t] = 1u;
+                atomicExch(p.fail_any, 1u);
+            }
+            return;
+        }
+        uint64_t vor = 0, vand = ~0ull;
+#pragma unroll 8
+        for (uint32_t i = tid; i < n; i += THREADS) {
+            const uint64_t c = __ldcg(src + i);
+            s_buf[i] = c;
+            vor |= c;
+            vand &= c;
+        }
+        block_or_and<THREADS>(vor, vand, sh.bs);  // barriers: the region is in s_buf
+        const uint64_t tau = block_topk_bound<THREADS>(s_buf, n, k, vor, vand, sh.bs,
+                                                       reinterpret_cast<uint32_t*>(s_buf + hist_off),
+                                                       s_buf + spill_off, &s_spill_n, &s_tau, p.err);
+        // The k selected entries go back to the region as output sort keys:
+        // slots from a block-wide scan of every thread's count, staged in
+        // shared memory (after the histograms) and copied out coalesced.
+        uint64_t* dst = p.cand + td.cbase;
+        uint64_t* stage = s_buf + hist_off;  // k <= cap - hist_off entries (checked below)
+        uint32_t nsel = 0;
+        for (uint32_t i = tid; i < n; i += THREADS) nsel += (s_buf[i] >= tau) ? 1u : 0u;
+        uint32_t total = 0;
+        uint32_t slot = block_exclusive_scan<THREADS>(nsel, &total, sh.bs);  // barriers: histograms no longer read
+        for (uint32_t i = tid; i < n; i += THREADS) {
+            const uint64_t c = s_buf[i];
+            if (c < tau) continue;
+            uint32_t pos = composite_pos(c);
+            if (pos >= static_cast<uint64_t>(tv.len)) {  // never expected; keep the gather in bounds
+                record_error(p.err, kErrBounds);
+                pos = 0;
+            }
+            uint64_t okey;
+            if constexpr (kScale) {
+                okey = output_sort_key(__float_as_uint(tv.data[pos]), pos, tv.sp, tv.ascend);
+            } else {
+                uint32_t key = static_cast<uint32_t>(c >> 32) ^ tv.sp.flip;  // key of the substituted value
+                if (!tv.ascend) key = ~key;
+                okey = (static_cast<uint64_t>(key) << 32) | pos;
+            }
+            if (slot < k) stage[slot] = okey;
+            else record_error(p.err, kErrInternal);
+            ++slot;
+        }
+        block_sync<THREADS>();
+        for (uint32_t i = tid; i < k; i += THREADS) dst[i] = stage[i];
+        if (tid == 0) {
+            if (total == k) p.rank_ready[t] = 1u;
+            else record_error(p.err, kErrInternal);
+        }
+        return;
+    }
     for (uint32_t b0 = 0; b0 < n;) {
         const uint32_t cnt = sh.cnt;
         const uint32_t take = min(n - b0, cap - cnt);  // > 0: cnt <= mid_keep < cap
@@ -56,6 +252,71 @@ __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, cons
         return;
     }
     finish_task<THREADS, !kScale>(p, tv, s_buf, k, sh);
+}
+
+// Output rows of the tasks whose k selected output keys merge_topk_kernel
+// left in their candidate regions: block (x, y) places keys
+// x * kRankPerBlock .. (x + 1) * kRankPerBlock - 1 of task merge_tasks[y].  A key's place in the row is the
+// number of the task's k keys below it (keys are unique); kRankSplit threads
+// count it over interleaved pairs of keys in shared memory and the first
+// writes the value and index there.
+template <bool kScale>
+__global__ void __launch_bounds__(kRankThreads) rank_write_kernel(FusedParams p, const int32_t* merge_tasks) {
+    extern __shared__ __align__(16) uint64_t s_keys[];
+    const int tid = threadIdx.x;
+    const int t = merge_tasks[blockIdx.y];
+    const uint32_t ready = __ldcg(p.rank_ready + t);
+    const FusedTask td = p.tasks[t];
+    if (ready == 0u) return;
+    const TaskView tv = task_view<kScale>(p, t, td);
+    const uint32_t k = tv.k;
+    const uint32_t q0 = blockIdx.x * kRankPerBlock;
+    if (q0 >= k || k > kRankMaxK) return;
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
+    const uint32_t k2 = (k + 1) & ~1u;  // an even count: a padding key ~0 ranks above every real key
+    for (uint32_t i = tid; i < k2; i += kRankThreads) s_keys[i] = i < k ? __ldcg(src + i) : ~0ull;
+    __syncthreads();
+    const uint32_t q = q0 + static_cast<uint32_t>(tid) / kRankSplit;
+    const uint32_t part = static_cast<uint32_t>(tid) % kRankSplit;
+    const uint64_t x = q < k ? s_keys[q] : ~0ull;
+    const ulonglong2* pairs = reinterpret_cast<const ulonglong2*>(s_keys);
+    uint32_t c0 = 0, c1 = 0;
+    // Pairs part, part + kRankSplit, ...: the threads of a key read
+    // consecutive bytes, and the other key of the warp reads the same ones.
+#pragma unroll 4
+    for (uint32_t i = part; i < k2 / 2; i += kRankSplit) {
+        const ulonglong2 y = pairs[i];
+        c0 += (y.x < x) ? 1u : 0u;
+        c1 += (y.y < x) ? 1u : 0u;
+    }
+    uint32_t c = c0 + c1;
+#pragma unroll
+    for (int m = 1; m < kRankSplit; m <<= 1) c += __shfl_xor_sync(kFullMask, c, m);
+    if (part != 0u || q >= k) return;
+    if (c >= k) {  // never expected: keys are unique
+        record_error(p.err, kErrInternal);
+        return;
+    }
+    const uint32_t pos = static_cast<uint32_t>(x);
+    float val;
+    if constexpr (kScale) {
+        val = tv.data[pos];
+    } else {
+        uint32_t key = static_cast<uint32_t>(x >> 32);
+        if (!tv.ascend) key = ~key;
+        val = (key == key_of_bits(tv.sp.nan_bits)) ? tv.data[pos]
+                                                   : __uint_as_float((key & 0x80000000u) ? (key ^ 0x80000000u) : ~key);
+    }
+    int64_t idx;
+    if (tv.iin) {
+        idx = (p.idx_bytes == 8) ? static_cast<const int64_t*>(tv.iin)[pos]
+                                 : static_cast<int64_t>(static_cast<const int32_t*>(tv.iin)[pos]);
+    } else {
+        idx = static_cast<int64_t>(pos) + 1;  // 1-based position (filter.jl:76-77)
+    }
+    tv.vout[c] = val;
+    if (p.idx_bytes == 8) static_cast<int64_t*>(tv.iout)[c] = idx;
+    else static_cast<int32_t*>(tv.iout)[c] = static_cast<int32_t>(idx);
 }
 
 }  // namespace radik

@@ -265,3 +265,29 @@ def test_many_items_per_block(oracle, radik, torch_cuda, monkeypatch, form):
     for k in (16, 256):
         _compare(oracle, radik, torch_cuda, w, [1 << 20], k)
         _compare(oracle, radik, torch_cuda, w, [300_000, 1 << 19, 5], k, largest=False)
+
+
+@pytest.mark.parametrize("k", [256, 1000, 4096, 6000, 8192])
+def test_flush_merge_and_rank_paths(oracle, radik, torch_cuda, monkeypatch, k):
+    """A task split into 32 segments with a sampled threshold runs in flush
+    mode; its merge selects in registers and leaves the row to the rank
+    kernel when the candidates fit (up to 16384), else selects, sorts and
+    writes in one block.  Both must give the exact answer with ties at the
+    k-th value, NaN, custom indices and scaling."""
+    monkeypatch.setenv("RADIK_SEG", "65536")
+    n = 1 << 21 if k <= 1000 else 1 << 24  # the block sampler's rank stays within its limit
+    rng = np.random.default_rng(k)
+    x = rng.standard_normal(n).astype(np.float32)
+    ws = radik.RadiKWorkspace("cuda", n, 1)
+    ws.prepare([n], k)
+    assert ws.plan_info()["sample_jobs"] > 0  # flush mode with the merge and rank kernels
+    ws.close()
+    _compare(oracle, radik, torch_cuda, x, [n], k)
+    _compare(oracle, radik, torch_cuda, x, [n], k, largest=False, rev=True)
+    q = np.round(x * 64.0).astype(np.float32) / 64.0  # about 500 distinct values: ties at the k-th one
+    q[::1009] = np.nan
+    _compare(oracle, radik, torch_cuda, q, [n], k, largest=False)
+    _compare(oracle, radik, torch_cuda, q, [n], k, rev=True)
+    ind = rng.permutation(n).astype(np.int64) * 5 - 7
+    _compare(oracle, radik, torch_cuda, x, [n], k, indices=ind)
+    _compare(oracle, radik, torch_cuda, x + 2.5, [n], k, withscale=True, largest=False)
