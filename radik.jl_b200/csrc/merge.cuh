@@ -30,121 +30,6 @@ constexpr int kRankThreads = 256;      // rank_write_kernel: threads per block
 constexpr int kRankSplit = 16;         // threads counting for one output key
 constexpr int kRankPerBlock = kRankThreads / kRankSplit;  // output keys placed per block
 
-constexpr uint32_t kWarpBisect = 512;  // boundary-bin entries one warp finishes (16 per lane)
-
-// Bound of the k best among buf[0, n) (unique composites in shared memory,
-// 1 <= k <= n; vor and vand span them).  8-bit digit windows below the
-// common prefix narrow the entries in play to the bin holding rank k: every
-// warp counts into its own histogram (whist, 256 words per warp: no
-// contention between warps on the few bins that most entries fall into), the
-// histograms are summed and searched for rank k.  Once that bin holds at
-// most kWarpBisect entries they are copied to `spill` and warp 0 finds the
-// exact bound by bisection over their bits.  Returns tau with exactly k
-// entries >= tau.  All threads call.
-template <int THREADS>
-__device__ uint64_t block_topk_bound(const uint64_t* buf, uint32_t n, uint32_t k, uint64_t vor, uint64_t vand,
-                                     BlockScratch<THREADS>& s, uint32_t* whist, uint64_t* spill, uint32_t* spill_n,
-                                     unsigned long long* result, uint32_t* err) {
-    constexpr int W = 8;
-    const uint32_t tid = threadIdx.x, lane = tid & 31u;
-    const uint64_t diff = vor ^ vand;
-    if (diff == 0ull) return vand;  // a single entry
-    int top = 63 - __clzll(static_cast<long long>(diff));
-    uint64_t prefix = (top >= 63) ? 0ull : (vand >> (top + 1));
-    int pbits = 63 - top;  // bits above `top` shared by the entries still in play
-    uint32_t r = k;
-    for (int guard = 0; guard < 9; ++guard) {
-        const int w = top + 1 < W ? top + 1 : W;
-        const int sh = top + 1 - w;
-        const uint32_t nb = 1u << w;
-        uint32_t* my = whist + (tid >> 5) * 256u;
-        for (uint32_t i = lane; i < nb; i += 32) my[i] = 0;
-        __syncwarp();
-        for (uint32_t i = tid; i < n; i += THREADS) {
-            const uint64_t c = buf[i];
-            if (pbits == 0 || (c >> (sh + w)) == prefix) atomicAdd(my + (static_cast<uint32_t>(c >> sh) & (nb - 1)), 1u);
-        }
-        block_sync<THREADS>();
-        for (uint32_t i = tid; i < nb; i += THREADS) {
-            uint32_t sum = 0;
-#pragma unroll 8
-            for (int ww = 0; ww < THREADS / 32; ++ww) sum += whist[ww * 256 + i];
-            s.hist[i] = sum;
-        }
-        block_sync<THREADS>();
-        block_rank_search<THREADS>(r, nb, s);
-        const uint32_t b = s.bc32[0], rr = s.bc32[1], cb = s.bc32[2];
-        block_sync<THREADS>();  // hist and bc32 are rewritten by the next window
-        if (cb == 0xffffffffu) {  // never expected: rank k lies beyond the entries
-            if (tid == 0) record_error(err, kErrInternal);
-            return vand;
-        }
-        const uint64_t bin_prefix = (pbits == 0) ? b : ((prefix << w) | b);
-        if (cb == rr || sh == 0) return bin_prefix << sh;  // the whole bin is in: k entries >= its lower edge
-        if (cb <= kWarpBisect) {
-            // The boundary bin to `spill`; warp 0 finds its rr-th largest.
-            if (tid == 0) *spill_n = 0;
-            block_sync<THREADS>();
-            const uint32_t lt = lanemask_lt();
-            for (uint32_t base = 0; base < n; base += THREADS) {
-                const uint32_t i = base + tid;
-                const uint64_t c = i < n ? buf[i] : 0ull;
-                const bool in = i < n && (c >> sh) == bin_prefix;
-                const uint32_t m = __ballot_sync(kFullMask, in);
-                if (m == 0u) continue;
-                const uint32_t leader = __ffs(m) - 1;
-                uint32_t o = 0;
-                if (lane == leader) o = atomicAdd(spill_n, __popc(m));
-                o = __shfl_sync(kFullMask, o, leader);
-                if (in && o + __popc(m & lt) < kWarpBisect) spill[o + __popc(m & lt)] = c;
-            }
-            block_sync<THREADS>();
-            if (tid < 32) {
-                const uint32_t cnt = *spill_n < kWarpBisect ? *spill_n : kWarpBisect;
-                uint64_t wor = 0, wand = ~0ull;
-                for (uint32_t i = lane; i < cnt; i += 32) {
-                    wor |= spill[i];
-                    wand &= spill[i];
-                }
-#pragma unroll
-                for (int m = 16; m > 0; m >>= 1) {
-                    wor |= __shfl_xor_sync(kFullMask, wor, m);
-                    wand &= __shfl_xor_sync(kFullMask, wand, m);
-                }
-                uint64_t tau = wand;
-                const uint64_t d = wor ^ wand;
-                if (d != 0ull && rr <= cnt) {
-                    int bb = 63 - __clzll(static_cast<long long>(d));
-                    tau = (bb == 63) ? 0ull : (wand & ~((2ull << bb) - 1));
-                    uint32_t cge = cnt;
-                    for (; bb >= 0 && cge != rr; --bb) {
-                        const uint64_t cand = tau | (1ull << bb);
-                        uint32_t c = 0;
-                        for (uint32_t i = lane; i < cnt; i += 32) c += (spill[i] >= cand) ? 1u : 0u;
-                        c = __reduce_add_sync(kFullMask, c);
-                        if (c >= rr) {
-                            tau = cand;
-                            cge = c;
-                        }
-                    }
-                }
-                if (lane == 0) {
-                    if (cnt != cb) record_error(err, kErrInternal);
-                    *result = tau;
-                }
-            }
-            block_sync<THREADS>();
-            return *result;
-        }
-        prefix = bin_prefix;
-        pbits += w;
-        r = rr;
-        top = sh - 1;
-    }
-    if (tid == 0) record_error(err, kErrInternal);
-    return prefix;
-}
-
 template <int THREADS, bool kScale>
 __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, const int32_t* merge_tasks) {
     extern __shared__ __align__(16) uint64_t s_buf[];
