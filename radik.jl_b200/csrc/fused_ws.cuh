@@ -12,10 +12,10 @@
 //     is paid once per 32 elements; the warp frees the stage ("empty"
 //     mbarrier) as soon as it is done with it, and no barrier is shared
 //     between warps while they stream;
-//   * the fast test keeps one bit per lane and float4; only lanes with a
-//     passing group compute element bits, one warp scan places the warp's
-//     candidates in its own region, and the values are read back from the
-//     stage the warp still holds;
+//   * the fast test keeps one bit per element (the float compare against
+//     the threshold's value, on the registers it loaded); one warp scan
+//     places the warp's candidates in its own region, and their values are
+//     read back from the stage the warp still holds;
 //   * when a warp's region overflows it keeps the tile, raises a request and
 //     every consumer warp joins a block-wide shrink (polling the request
 //     between tiles and while waiting for one), after which the requester
@@ -198,19 +198,27 @@ __device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, u
         mbar_wait_bounded(full + j % STAGES, (j / STAGES) & 1u, kWaitPolls);
 }
 
-// Fast test of a warp tile: bit j of the result is set when some element of
-// this lane's float4 j passes the fast filter.  Float4 j of the lane is
-// src[j * 32 + lane]; only the first nv float4 of the tile are elements.
+// Fast test of a warp tile: bit 4 j + e of the result is set when component
+// e of this lane's float4 j passes the fast filter (the float compare against
+// the threshold's value).  Float4 j of the lane is src[j * 32 + lane]; only
+// the first nv float4 of the tile are elements: the others read as ff.pad4
+// and their bits are cleared (pad4 passes when the threshold is -inf).
 template <int J, bool kScale>
-__device__ __forceinline__ uint32_t ws_group_mask(const float4* src, uint32_t nv, uint32_t lane, const FastFilter& ff,
-                                                  float scaler) {
+__device__ __forceinline__ uint32_t ws_elem_mask(const float4* src, uint32_t nv, uint32_t lane, const FastFilter& ff,
+                                                 float scaler) {
     float4 x[J];
+    uint32_t valid = 0xffffffffu;
     if (nv >= 32u * J) {
 #pragma unroll
         for (int j = 0; j < J; ++j) x[j] = src[j * 32 + lane];
     } else {
+        valid = 0;
 #pragma unroll
-        for (int j = 0; j < J; ++j) x[j] = (j * 32 + lane < nv) ? src[j * 32 + lane] : ff.pad4;
+        for (int j = 0; j < J; ++j) {
+            const bool in = j * 32 + lane < nv;
+            x[j] = in ? src[j * 32 + lane] : ff.pad4;
+            valid |= in ? (0xfu << (4 * j)) : 0u;
+        }
     }
     if constexpr (kScale) {
 #pragma unroll
@@ -219,57 +227,48 @@ __device__ __forceinline__ uint32_t ws_group_mask(const float4* src, uint32_t nv
             x[j].z = __fsub_rn(x[j].z, scaler); x[j].w = __fsub_rn(x[j].w, scaler);
         }
     }
-    uint32_t gm = 0;
+    uint32_t em = 0;
     if (ff.dir == 0u && !ff.nan_pass) {
 #pragma unroll
         for (int j = 0; j < J; ++j)
-            gm |= static_cast<uint32_t>((x[j].x >= ff.t) | (x[j].y >= ff.t) | (x[j].z >= ff.t) | (x[j].w >= ff.t)) << j;
+            em |= (static_cast<uint32_t>(x[j].x >= ff.t) | (static_cast<uint32_t>(x[j].y >= ff.t) << 1) |
+                   (static_cast<uint32_t>(x[j].z >= ff.t) << 2) | (static_cast<uint32_t>(x[j].w >= ff.t) << 3))
+                  << (4 * j);
     } else if (!ff.nan_pass) {
 #pragma unroll
         for (int j = 0; j < J; ++j)
-            gm |= static_cast<uint32_t>((x[j].x <= ff.tr) | (x[j].y <= ff.tr) | (x[j].z <= ff.tr) | (x[j].w <= ff.tr))
-                  << j;
+            em |= (static_cast<uint32_t>(x[j].x <= ff.tr) | (static_cast<uint32_t>(x[j].y <= ff.tr) << 1) |
+                   (static_cast<uint32_t>(x[j].z <= ff.tr) << 2) | (static_cast<uint32_t>(x[j].w <= ff.tr) << 3))
+                  << (4 * j);
     } else if (ff.dir == 0u) {
 #pragma unroll
         for (int j = 0; j < J; ++j)
-            gm |= static_cast<uint32_t>(!(x[j].x < ff.t) | !(x[j].y < ff.t) | !(x[j].z < ff.t) | !(x[j].w < ff.t)) << j;
+            em |= (static_cast<uint32_t>(!(x[j].x < ff.t)) | (static_cast<uint32_t>(!(x[j].y < ff.t)) << 1) |
+                   (static_cast<uint32_t>(!(x[j].z < ff.t)) << 2) | (static_cast<uint32_t>(!(x[j].w < ff.t)) << 3))
+                  << (4 * j);
     } else {
 #pragma unroll
         for (int j = 0; j < J; ++j)
-            gm |= static_cast<uint32_t>(!(x[j].x > ff.tr) | !(x[j].y > ff.tr) | !(x[j].z > ff.tr) | !(x[j].w > ff.tr))
-                  << j;
+            em |= (static_cast<uint32_t>(!(x[j].x > ff.tr)) | (static_cast<uint32_t>(!(x[j].y > ff.tr)) << 1) |
+                   (static_cast<uint32_t>(!(x[j].z > ff.tr)) << 2) | (static_cast<uint32_t>(!(x[j].w > ff.tr)) << 3))
+                  << (4 * j);
     }
-    return gm;
+    return em & valid;
 }
 
 // Places candidates of a warp tile in the warp's region.  Element bit
 // b = 4 j + e of a lane is component e of its float4 j (src[j * 32 + lane]).
-// `groups` selects float4 whose elements are tested with the fast filter
-// (initial placement); with groups == 0, `elems` lists elements offered again
-// after a shrink, kept only if their composite beats thr.  One warp scan
-// gives every lane its slots; returns the element bits that found no room.
+// `elems` lists this lane's elements: from the fast filter (exact == false,
+// placed as they are) or offered again after a shrink (exact == true, kept
+// only if their composite beats thr).  One warp scan gives every lane its
+// slots; returns the element bits that found no room.
 template <int J, bool kScale>
-__device__ __forceinline__ uint32_t ws_place(const float4* src, uint32_t groups, uint32_t elems, uint32_t nv,
-                                             uint32_t qb, uint32_t pos0, uint64_t thr, const FastFilter& ff,
-                                             float scaler, const ScoreParams& sp, uint64_t* region, uint32_t R,
-                                             uint32_t& wcnt, uint32_t lane) {
+__device__ __forceinline__ uint32_t ws_place(const float4* src, uint32_t elems, bool exact, uint32_t qb, uint32_t pos0,
+                                             uint64_t thr, float scaler, const ScoreParams& sp, uint64_t* region,
+                                             uint32_t R, uint32_t& wcnt, uint32_t lane) {
     const float* srcf = reinterpret_cast<const float*>(src);
     uint32_t pm = elems;
-    for (uint32_t gs = groups; gs; gs &= gs - 1) {
-        const int j = __ffs(gs) - 1;
-        if (j * 32 + lane >= nv) continue;  // past the end of the segment
-        const float4 f = src[j * 32 + lane];
-        const float fv[4] = {f.x, f.y, f.z, f.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            float x = fv[e];
-            if constexpr (kScale) x = __fsub_rn(x, scaler);
-            const float xs = __uint_as_float(__float_as_uint(x) ^ ff.dir);
-            const bool ps = ff.nan_pass ? !(xs < ff.t) : (xs >= ff.t);
-            pm |= static_cast<uint32_t>(ps) << (j * 4 + e);
-        }
-    }
-    if (groups == 0u) {  // offered again: exact test against the raised threshold
+    if (exact) {
         uint32_t keep = 0;
         for (uint32_t m = pm; m; m &= m - 1) {
             const int b = __ffs(m) - 1;
@@ -516,8 +515,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                             const uint32_t st = gt % STAGES;
                             const float4* src = from_ring ? ring4 + static_cast<size_t>(st) * TW4 : gsrc + i * TW4;
                             const uint32_t qb = i * TW4;
-                            om = ws_place<J, kScale>(src, 0u, om, nvec - qb, qb, pos0, thr, ff, scaler, tv.sp, region,
-                                                     R, wcnt, lane);
+                            om = ws_place<J, kScale>(src, om, true, qb, pos0, thr, scaler, tv.sp, region, R, wcnt,
+                                                     lane);
                             if (__any_sync(kFullMask, om != 0u)) {
                                 if (lane == 0) st_volatile_u32(&sh.req, 1u);
                             } else {
@@ -560,18 +559,18 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                         }
                         const uint32_t qb = i * TW4;
                         const uint32_t nv = nvec - qb < TW4 ? nvec - qb : TW4;
-                        const uint32_t gm = ws_group_mask<J, kScale>(src, nv, lane, ff, scaler);
-                        if (__any_sync(kFullMask, gm != 0u)) {
-                            om = ws_place<J, kScale>(src, gm, 0u, nv, qb, pos0, thr, ff, scaler, tv.sp, region, R,
-                                                     wcnt, lane);
+                        const uint32_t em = ws_elem_mask<J, kScale>(src, nv, lane, ff, scaler);
+                        if (__any_sync(kFullMask, em != 0u)) {
+                            om = ws_place<J, kScale>(src, em, false, qb, pos0, thr, scaler, tv.sp, region, R, wcnt,
+                                                     lane);
                             if (flush) {
                                 // Write the region out and place the rest (bounded:
                                 // each round places up to R of at most 32 * 4 * J).
                                 for (int rounds = 0; rounds < 64 && __any_sync(kFullMask, om != 0u); ++rounds) {
                                     ws_flush(region, wcnt, R, fdst, p.task_cnt + t, fcap, p.fail + t, p.fail_any,
                                              lane);
-                                    om = ws_place<J, kScale>(src, 0u, om, nvec - qb, qb, pos0, thr, ff, scaler, tv.sp,
-                                                             region, R, wcnt, lane);
+                                    om = ws_place<J, kScale>(src, om, true, qb, pos0, thr, scaler, tv.sp, region, R,
+                                                             wcnt, lane);
                                 }
                             } else if (__any_sync(kFullMask, om != 0u)) {
                                 if (lane == 0) st_volatile_u32(&sh.req, 1u);
