@@ -127,6 +127,10 @@ MergeKernel pick_merge(bool scale) {
     return scale ? merge_topk_kernel<kMergeThreads, true> : merge_topk_kernel<kMergeThreads, false>;
 }
 MergeKernel pick_rank(bool scale) { return scale ? rank_write_kernel<true> : rank_write_kernel<false>; }
+constexpr int kDeferThreads = 128;  // merge blocks of deferred tasks (k up to the streaming buffer)
+MergeKernel pick_defer(bool scale) {
+    return scale ? merge_topk_kernel<kDeferThreads, true> : merge_topk_kernel<kDeferThreads, false>;
+}
 constexpr size_t kRankSmem = sizeof(uint64_t) * (kRankMaxK + 2);
 
 using SampleKernel = void (*)(FusedParams, const SampleJob*, uint64_t*, uint32_t*);
@@ -143,7 +147,8 @@ int env_int(const char* name, int dflt) {
 // Tunable shape of a plan.  Defaults are the measured best for the common
 // cases; radik_ws_autotune picks another per batch shape; environment
 // variables (RADIK_WS, RADIK_WST, RADIK_WSJ, RADIK_WSS, RADIK_WS_SAMPLE,
-// RADIK_WS_WINDOWS, RADIK_SEG_DIV) override both, for experiments.
+// RADIK_WS_WINDOWS, RADIK_SEG_DIV, RADIK_DEFER) override both, for
+// experiments.
 struct TuneConfig {
     int form = -1;          // -1 automatic, 0 barrier form, 1 warp-specialised form
     int ws_threads = 128;   // warp-specialised: consumer threads
@@ -152,9 +157,11 @@ struct TuneConfig {
     int sample_max = 2048;  // single-segment sample (elements)
     int sample_windows = 2; // digit windows of its rank threshold
     int seg_div = 3;        // work items per resident block when splitting tasks
+    int defer = -1;         // single-segment tasks finished by a merge kernel: -1 automatic, 0 no, 1 yes
     bool operator==(const TuneConfig& o) const {
         return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
-               sample_max == o.sample_max && sample_windows == o.sample_windows && seg_div == o.seg_div;
+               sample_max == o.sample_max && sample_windows == o.sample_windows && seg_div == o.seg_div &&
+               defer == o.defer;
     }
 };
 
@@ -166,6 +173,7 @@ TuneConfig with_env(TuneConfig c) {
     c.sample_max = env_int("RADIK_WS_SAMPLE", c.sample_max);
     c.sample_windows = env_int("RADIK_WS_WINDOWS", c.sample_windows);
     c.seg_div = std::max(1, env_int("RADIK_SEG_DIV", c.seg_div));
+    c.defer = env_int("RADIK_DEFER", c.defer);
     if (c.sample_max != 2048 && c.sample_max != 4096) c.sample_max = 2048;
     return c;
 }
@@ -213,6 +221,9 @@ struct Plan {
     std::vector<FusedSeg> segs;
     std::vector<SampleJob> jobs;
     std::vector<int32_t> merge_tasks;
+    // Deferred single-segment tasks (their rows written by the 128-thread merge).
+    std::vector<int32_t> defer_tasks;
+    size_t defer_off = 0;
 };
 
 struct radik_ws {
@@ -475,6 +486,31 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
                 np.tasks[t].flags |= kTaskFlush;
                 np.merge_tasks.push_back(static_cast<int32_t>(t));
             }
+    // Deferred finish: when a batch has enough single-segment tasks to give
+    // every block several (three or more: measured, the separate pass costs
+    // more than it overlaps below that), their blocks leave the candidates
+    // in a region of cap entries and take the next task; a merge kernel (one
+    // 128-thread block per task) finishes them all at once.
+    np.defer_tasks.clear();
+    if (np.fused && np.ws_form && tc.defer != 0) {
+        std::vector<int32_t> elig;
+        for (int64_t t = 0; t < T; ++t) {
+            const FusedTask& td = np.tasks[t];
+            if (td.nseg == 1 && td.len > static_cast<int64_t>(kk) && td.len >= 16384 && (td.flags & kTaskSampled) == 0)
+                elig.push_back(static_cast<int32_t>(t));
+        }
+        const bool want = tc.defer > 0 || static_cast<int64_t>(elig.size()) >= 3 * resident;
+        if (want && !elig.empty() &&
+            set_smem_and_occupancy(reinterpret_cast<const void*>(pick_defer(scale)), kDeferThreads,
+                                   static_cast<size_t>(np.cap) * 8) >= 1) {
+            for (int32_t t : elig) {
+                np.tasks[t].flags |= kTaskDefer;
+                np.tasks[t].cbase = np.cand_entries;
+                np.cand_entries += np.cap;
+            }
+            np.defer_tasks = std::move(elig);
+        }
+    }
     np.grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(np.nsegs, resident)));
     const int grid_cap = env_int("RADIK_GRID", 0);  // fewer CTAs than resident (tests: many items per CTA)
     if (grid_cap > 0 && np.fused) np.grid = std::min(np.grid, grid_cap);
@@ -495,12 +531,13 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     np.segs_off = round_up(sizeof(FusedTask) * T, 256);
     np.jobs_off = np.segs_off + round_up(sizeof(FusedSeg) * np.segs.size(), 256);
     np.merge_off = np.jobs_off + round_up(sizeof(SampleJob) * np.jobs.size(), 256);
+    np.defer_off = np.merge_off + round_up(sizeof(int32_t) * np.merge_tasks.size(), 256);
     np.valid = true;
     return RADIK_OK;
 }
 
-// Size of the descriptor block (tasks, segments, sample jobs, merge list) of a plan.
-size_t plan_desc_bytes(const Plan& pl) { return pl.merge_off + sizeof(int32_t) * pl.merge_tasks.size(); }
+// Size of the descriptor block (tasks, segments, sample jobs, merge lists) of a plan.
+size_t plan_desc_bytes(const Plan& pl) { return pl.defer_off + sizeof(int32_t) * pl.defer_tasks.size(); }
 
 // Build the launch plan for a batch shape and size the workspace for it.
 // Key of a call's plan: the batch shape and the configuration that applies
@@ -551,8 +588,8 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     if (e == cudaSuccess && np.fused) {
         e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.cand_entries));
         if (e == cudaSuccess) e = ws->samples.ensure(sizeof(uint64_t) * static_cast<size_t>(np.sample_entries));
-        const size_t sort_blocks = std::max<size_t>(
-            {static_cast<size_t>(np.grid), static_cast<size_t>(np.retry_grid), np.merge_tasks.size()});
+        const size_t sort_blocks = std::max<size_t>({static_cast<size_t>(np.grid), static_cast<size_t>(np.retry_grid),
+                                                     np.merge_tasks.size(), np.defer_tasks.size()});
         if (e == cudaSuccess && kk > kBitonicMax)
             e = ws->scratch.ensure(sizeof(uint64_t) * sort_blocks * kk);
     }
@@ -588,6 +625,9 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
             if (!np.merge_tasks.empty())
                 std::memcpy(ws->h_stage + np.merge_off, np.merge_tasks.data(),
                             sizeof(int32_t) * np.merge_tasks.size());
+            if (!np.defer_tasks.empty())
+                std::memcpy(ws->h_stage + np.defer_off, np.defer_tasks.data(),
+                            sizeof(int32_t) * np.defer_tasks.size());
             e = cudaMemcpyAsync(ws->desc.p, ws->h_stage, desc_bytes, cudaMemcpyHostToDevice, upload);
         }
         if (e == cudaSuccess) e = cudaMemsetAsync(ws->state.p, 0, L.bytes, upload);
@@ -602,6 +642,9 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
         if (e == cudaSuccess && !np.merge_tasks.empty())
             e = cudaMemcpy(ws->desc.as<char>(np.merge_off), np.merge_tasks.data(),
                            sizeof(int32_t) * np.merge_tasks.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !np.defer_tasks.empty())
+            e = cudaMemcpy(ws->desc.as<char>(np.defer_off), np.defer_tasks.data(),
+                           sizeof(int32_t) * np.defer_tasks.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, L.bytes);
     }
     if (e == cudaSuccess && np.fused && !np.jobs.empty()) {
@@ -680,6 +723,15 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
                          static_cast<unsigned>(pl.merge_tasks.size()));
         const size_t rsmem = sizeof(uint64_t) * (std::min<size_t>(p.kmax, kRankMaxK) + 2);
         pick_rank(scale)<<<rgrid, kRankThreads, rsmem, s>>>(m, ws->desc.as<int32_t>(pl.merge_off));
+        RADIK_CUDA(cudaGetLastError());
+    }
+    if (!pl.defer_tasks.empty()) {
+        // Deferred tasks: one 128-thread block each selects, sorts and writes.
+        FusedParams d = p;
+        d.cap = pl.cap;
+        d.rank_ready = nullptr;
+        pick_defer(scale)<<<static_cast<unsigned>(pl.defer_tasks.size()), kDeferThreads,
+                            static_cast<size_t>(pl.cap) * 8, s>>>(d, ws->desc.as<int32_t>(pl.defer_off));
         RADIK_CUDA(cudaGetLastError());
     }
     if (!pl.jobs.empty()) {
@@ -897,7 +949,9 @@ int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
     // fused: sampling kernel + fused kernel (+ merge kernel for flush-mode
     // tasks) + retry launch when sampled;
     // multi-pass: histogram, select, compact, advance, finalize at least.
-    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) : 5;
+    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) +
+                                           (pl.defer_tasks.empty() ? 0 : 1)
+                                     : 5;
     return RADIK_OK;
 }
 
@@ -983,6 +1037,8 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     { TuneConfig c = d; c.form = 0; cands.push_back(c); }
     { TuneConfig c = d; c.seg_div = 2; cands.push_back(c); }
     { TuneConfig c = d; c.seg_div = 6; cands.push_back(c); }
+    { TuneConfig c = d; c.defer = 0; cands.push_back(c); }
+    { TuneConfig c = d; c.defer = 1; cands.push_back(c); }
     PlanKey base = plan_key(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
     auto set_choice = [&](const TuneConfig& c) {
         for (auto& e : ws->tuned) {
@@ -1190,7 +1246,9 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
     view.n = maxlen;
     view.num_tasks = num_tasks;
     view.index_bytes = idx_bytes;
-    rc = plan_shape(h_task_lens, num_tasks, k, flags, view.plan, with_env(TuneConfig{}));
+    TuneConfig tc = with_env(TuneConfig{});
+    tc.defer = 0;  // deferred regions are sized for a workspace, not for the static scratch
+    rc = plan_shape(h_task_lens, num_tasks, k, flags, view.plan, tc);
     if (rc) return rc;
     const Plan& pl = view.plan;
     if (!pl.fused) return fail(RADIK_ERR_WS_TOO_SMALL, "the fused kernel's candidate buffer does not fit for this k");
@@ -1231,6 +1289,9 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
     if (!pl.merge_tasks.empty())
         RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.merge_off), pl.merge_tasks.data(),
                                    sizeof(int32_t) * pl.merge_tasks.size(), cudaMemcpyHostToDevice, s));
+    if (!pl.defer_tasks.empty())
+        RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.defer_off), pl.defer_tasks.data(),
+                                   sizeof(int32_t) * pl.defer_tasks.size(), cudaMemcpyHostToDevice, s));
     FusedParams p = fused_params(&view, d_val_out, d_idx_out, idx_bytes, d_val_in, d_idx_in, k, flags);
     rc = run_fused(&view, p, flags, s);
     if (rc) return rc;

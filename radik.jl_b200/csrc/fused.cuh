@@ -38,7 +38,10 @@ namespace radik {
 // kTaskFlush: a sampled task split into segments whose candidates go straight
 // to its candidate region (no per-segment selection); the merge kernel
 // (merge.cuh) finishes it.
-enum : uint32_t { kTaskLargest = 1u, kTaskAscend = 2u, kTaskSampled = 4u, kTaskFlush = 8u };
+// kTaskDefer: a single-segment task whose streaming block leaves its
+// candidates in the task's region (p.cap entries) for the merge kernel to
+// finish, so that the block moves on to its next task at once.
+enum : uint32_t { kTaskLargest = 1u, kTaskAscend = 2u, kTaskSampled = 4u, kTaskFlush = 8u, kTaskDefer = 16u };
 
 struct FusedTask {
     int64_t start;   // global offset of the task in p.data (uniform-input mode)

@@ -619,6 +619,14 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
 
             if (flush) {
                 // merge.cuh selects the task's k best from its candidate region.
+            } else if (!multi && (td.flags & kTaskDefer) != 0u && !p.retry) {
+                // Deferred finish: the candidates (at least min(len, k), all in
+                // [0, sh.f.cnt) after the gather) to the task's region; the
+                // merge kernel selects, sorts and writes the row.
+                const uint32_t cnt = buffer_count<THREADS>(p, sh.f);
+                uint64_t* dst = p.cand + td.cbase;
+                for (uint32_t i = tid; i < cnt; i += THREADS) dst[i] = s_buf[i];
+                if (tid == 0) p.task_cnt[t] = cnt;
             } else if (!multi) {
                 uint64_t kth = 0;
                 const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;

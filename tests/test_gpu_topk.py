@@ -225,10 +225,12 @@ KERNEL_FORMS = [
     {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "8"},
     {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "12", "RADIK_WS_SAMPLE": "4096",
      "RADIK_WS_WINDOWS": "3"},
+    {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "8", "RADIK_DEFER": "1"},
 ]
 
 
-@pytest.mark.parametrize("form", KERNEL_FORMS, ids=["barrier", "ws-256-j8", "ws-256-j4", "ws-128-s8", "ws-128-s12"])
+@pytest.mark.parametrize("form", KERNEL_FORMS, ids=["barrier", "ws-256-j8", "ws-256-j4", "ws-128-s8", "ws-128-s12",
+                                                    "ws-128-s8-defer"])
 def test_many_items_per_block(oracle, radik, torch_cuda, monkeypatch, form):
     """A grid of 2-3 blocks works through every batch, so each block takes
     many work items in a row: ring stages, phases and item slots carry over
@@ -291,3 +293,30 @@ def test_flush_merge_and_rank_paths(oracle, radik, torch_cuda, monkeypatch, k):
     ind = rng.permutation(n).astype(np.int64) * 5 - 7
     _compare(oracle, radik, torch_cuda, x, [n], k, indices=ind)
     _compare(oracle, radik, torch_cuda, x + 2.5, [n], k, withscale=True, largest=False)
+
+
+@pytest.mark.parametrize("k", [1, 64, 256, 1000, 5000])
+def test_deferred_finish(oracle, radik, torch_cuda, monkeypatch, k):
+    """Single-segment tasks whose streaming block leaves the candidates to
+    the 128-thread merge kernel (RADIK_DEFER=1): exact results for every
+    order, ties and NaN, scaling and custom indices, beside short tasks that
+    are finished in the streaming kernel."""
+    monkeypatch.setenv("RADIK_DEFER", "1")
+    monkeypatch.setenv("RADIK_WS", "1")
+    rng = np.random.default_rng(500 + k)
+    lens = [65536] * 24 + [16384, 40000, 100, 0, 3, 200_000, 70_001]
+    x = rng.standard_normal(sum(lens)).astype(np.float32)
+    ws = radik.RadiKWorkspace("cuda", max(lens), len(lens))
+    ws.prepare(lens, k)
+    info = ws.plan_info()
+    ws.close()
+    assert info["kernels_per_call"] >= 2, info  # the streaming kernel and the deferred merge
+    _compare(oracle, radik, torch_cuda, x, lens, k)
+    _compare(oracle, radik, torch_cuda, x, lens, k, largest=False, rev=True)
+    q = np.round(x * 8.0).astype(np.float32) / 8.0  # heavy ties
+    q[::997] = np.nan
+    _compare(oracle, radik, torch_cuda, q, lens, k, rev=True)
+    _compare(oracle, radik, torch_cuda, q, lens, k, largest=False)
+    ind = rng.permutation(sum(lens)).astype(np.int64) * 3 + 1
+    _compare(oracle, radik, torch_cuda, x, lens, k, indices=ind)
+    _compare(oracle, radik, torch_cuda, x + 5.0, lens, k, withscale=True)
