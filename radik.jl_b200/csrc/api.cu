@@ -127,10 +127,6 @@ MergeKernel pick_merge(bool scale) {
     return scale ? merge_topk_kernel<kMergeThreads, true> : merge_topk_kernel<kMergeThreads, false>;
 }
 MergeKernel pick_rank(bool scale) { return scale ? rank_write_kernel<true> : rank_write_kernel<false>; }
-constexpr int kDeferThreads = 128;  // merge blocks of deferred tasks (k up to the streaming buffer)
-MergeKernel pick_defer(bool scale) {
-    return scale ? merge_topk_kernel<kDeferThreads, true> : merge_topk_kernel<kDeferThreads, false>;
-}
 constexpr size_t kRankSmem = sizeof(uint64_t) * (kRankMaxK + 2);
 
 using SampleKernel = void (*)(FusedParams, const SampleJob*, uint64_t*, uint32_t*);
@@ -157,7 +153,7 @@ struct TuneConfig {
     int sample_max = 2048;  // single-segment sample (elements)
     int sample_windows = 2; // digit windows of its rank threshold
     int seg_div = 3;        // work items per resident block when splitting tasks
-    int defer = -1;         // single-segment tasks finished by a merge kernel: -1 automatic, 0 no, 1 yes
+    int defer = -1;         // deferred finish of single-segment tasks: -1 automatic, 0 no, 1 yes
     bool operator==(const TuneConfig& o) const {
         return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
                sample_max == o.sample_max && sample_windows == o.sample_windows && seg_div == o.seg_div &&
@@ -221,9 +217,8 @@ struct Plan {
     std::vector<FusedSeg> segs;
     std::vector<SampleJob> jobs;
     std::vector<int32_t> merge_tasks;
-    // Deferred single-segment tasks (their rows written by the 128-thread merge).
+    // Deferred single-segment tasks (finished by blocks with no streaming left).
     std::vector<int32_t> defer_tasks;
-    size_t defer_off = 0;
 };
 
 struct radik_ws {
@@ -257,7 +252,7 @@ namespace {
 struct StateLayout {
     // kAny: multi-pass path: some task still active; fused path: some task failed.
     static constexpr size_t kErr = 0, kWork = 4, kWorkRetry = 8, kAny = 12, kHeader = 16;
-    size_t gthr, gthr_r, done, done_r, cnt, cnt_r, fail, sdone, rk, bytes;
+    size_t gthr, gthr_r, done, done_r, cnt, cnt_r, fail, sdone, rk, dctr, dq, bytes;
     explicit StateLayout(int64_t T) {
         const size_t t8 = round_up(sizeof(uint64_t) * static_cast<size_t>(std::max<int64_t>(T, 1)), 16);
         const size_t t4 = round_up(sizeof(uint32_t) * static_cast<size_t>(std::max<int64_t>(T, 1)), 16);
@@ -270,7 +265,9 @@ struct StateLayout {
         fail = cnt_r + t4;
         sdone = fail + t4;
         rk = sdone + t4;
-        bytes = rk + t4;
+        dctr = rk + t4;   // deferred tasks queued / claimed
+        dq = dctr + 16;   // queue of deferred tasks
+        bytes = dq + t4;
     }
 };
 
@@ -486,11 +483,10 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
                 np.tasks[t].flags |= kTaskFlush;
                 np.merge_tasks.push_back(static_cast<int32_t>(t));
             }
-    // Deferred finish: when a batch has enough single-segment tasks to give
-    // every block several (three or more: measured, the separate pass costs
-    // more than it overlaps below that), their blocks leave the candidates
-    // in a region of cap entries and take the next task; a merge kernel (one
-    // 128-thread block per task) finishes them all at once.
+    // Deferred finish: when a batch has at least as many single-segment
+    // tasks as resident blocks, their blocks leave the candidates in a
+    // region of cap entries, queue the task and take the next one; blocks
+    // with no streaming left finish queued tasks while the others stream.
     np.defer_tasks.clear();
     if (np.fused && np.ws_form && tc.defer != 0) {
         std::vector<int32_t> elig;
@@ -499,10 +495,8 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
             if (td.nseg == 1 && td.len > static_cast<int64_t>(kk) && td.len >= 16384 && (td.flags & kTaskSampled) == 0)
                 elig.push_back(static_cast<int32_t>(t));
         }
-        const bool want = tc.defer > 0 || static_cast<int64_t>(elig.size()) >= 3 * resident;
-        if (want && !elig.empty() &&
-            set_smem_and_occupancy(reinterpret_cast<const void*>(pick_defer(scale)), kDeferThreads,
-                                   static_cast<size_t>(np.cap) * 8) >= 1) {
+        const bool want = tc.defer > 0 || static_cast<int64_t>(elig.size()) >= resident;
+        if (want && !elig.empty()) {
             for (int32_t t : elig) {
                 np.tasks[t].flags |= kTaskDefer;
                 np.tasks[t].cbase = np.cand_entries;
@@ -531,13 +525,12 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     np.segs_off = round_up(sizeof(FusedTask) * T, 256);
     np.jobs_off = np.segs_off + round_up(sizeof(FusedSeg) * np.segs.size(), 256);
     np.merge_off = np.jobs_off + round_up(sizeof(SampleJob) * np.jobs.size(), 256);
-    np.defer_off = np.merge_off + round_up(sizeof(int32_t) * np.merge_tasks.size(), 256);
     np.valid = true;
     return RADIK_OK;
 }
 
 // Size of the descriptor block (tasks, segments, sample jobs, merge lists) of a plan.
-size_t plan_desc_bytes(const Plan& pl) { return pl.defer_off + sizeof(int32_t) * pl.defer_tasks.size(); }
+size_t plan_desc_bytes(const Plan& pl) { return pl.merge_off + sizeof(int32_t) * pl.merge_tasks.size(); }
 
 // Build the launch plan for a batch shape and size the workspace for it.
 // Key of a call's plan: the batch shape and the configuration that applies
@@ -588,8 +581,8 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     if (e == cudaSuccess && np.fused) {
         e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.cand_entries));
         if (e == cudaSuccess) e = ws->samples.ensure(sizeof(uint64_t) * static_cast<size_t>(np.sample_entries));
-        const size_t sort_blocks = std::max<size_t>({static_cast<size_t>(np.grid), static_cast<size_t>(np.retry_grid),
-                                                     np.merge_tasks.size(), np.defer_tasks.size()});
+        const size_t sort_blocks = std::max<size_t>(
+            {static_cast<size_t>(np.grid), static_cast<size_t>(np.retry_grid), np.merge_tasks.size()});
         if (e == cudaSuccess && kk > kBitonicMax)
             e = ws->scratch.ensure(sizeof(uint64_t) * sort_blocks * kk);
     }
@@ -625,9 +618,6 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
             if (!np.merge_tasks.empty())
                 std::memcpy(ws->h_stage + np.merge_off, np.merge_tasks.data(),
                             sizeof(int32_t) * np.merge_tasks.size());
-            if (!np.defer_tasks.empty())
-                std::memcpy(ws->h_stage + np.defer_off, np.defer_tasks.data(),
-                            sizeof(int32_t) * np.defer_tasks.size());
             e = cudaMemcpyAsync(ws->desc.p, ws->h_stage, desc_bytes, cudaMemcpyHostToDevice, upload);
         }
         if (e == cudaSuccess) e = cudaMemsetAsync(ws->state.p, 0, L.bytes, upload);
@@ -642,9 +632,6 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
         if (e == cudaSuccess && !np.merge_tasks.empty())
             e = cudaMemcpy(ws->desc.as<char>(np.merge_off), np.merge_tasks.data(),
                            sizeof(int32_t) * np.merge_tasks.size(), cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && !np.defer_tasks.empty())
-            e = cudaMemcpy(ws->desc.as<char>(np.defer_off), np.defer_tasks.data(),
-                           sizeof(int32_t) * np.defer_tasks.size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemset(ws->state.p, 0, L.bytes);
     }
     if (e == cudaSuccess && np.fused && !np.jobs.empty()) {
@@ -691,6 +678,9 @@ FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, c
     p.cand = ws->cand.as<uint64_t>();
     p.sort_scratch = ws->scratch.as<uint64_t>();
     p.rank_ready = ws->state.as<uint32_t>(L.rk);
+    p.ndefer = static_cast<uint32_t>(pl.defer_tasks.size());
+    p.defer_ctr = ws->state.as<uint32_t>(L.dctr);
+    p.defer_q = pl.defer_tasks.empty() ? nullptr : ws->state.as<uint32_t>(L.dq);
     return p;
 }
 
@@ -723,15 +713,6 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
                          static_cast<unsigned>(pl.merge_tasks.size()));
         const size_t rsmem = sizeof(uint64_t) * (std::min<size_t>(p.kmax, kRankMaxK) + 2);
         pick_rank(scale)<<<rgrid, kRankThreads, rsmem, s>>>(m, ws->desc.as<int32_t>(pl.merge_off));
-        RADIK_CUDA(cudaGetLastError());
-    }
-    if (!pl.defer_tasks.empty()) {
-        // Deferred tasks: one 128-thread block each selects, sorts and writes.
-        FusedParams d = p;
-        d.cap = pl.cap;
-        d.rank_ready = nullptr;
-        pick_defer(scale)<<<static_cast<unsigned>(pl.defer_tasks.size()), kDeferThreads,
-                            static_cast<size_t>(pl.cap) * 8, s>>>(d, ws->desc.as<int32_t>(pl.defer_off));
         RADIK_CUDA(cudaGetLastError());
     }
     if (!pl.jobs.empty()) {
@@ -949,9 +930,7 @@ int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
     // fused: sampling kernel + fused kernel (+ merge kernel for flush-mode
     // tasks) + retry launch when sampled;
     // multi-pass: histogram, select, compact, advance, finalize at least.
-    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) +
-                                           (pl.defer_tasks.empty() ? 0 : 1)
-                                     : 5;
+    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) : 5;
     return RADIK_OK;
 }
 
@@ -1289,9 +1268,6 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
     if (!pl.merge_tasks.empty())
         RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.merge_off), pl.merge_tasks.data(),
                                    sizeof(int32_t) * pl.merge_tasks.size(), cudaMemcpyHostToDevice, s));
-    if (!pl.defer_tasks.empty())
-        RADIK_CUDA(cudaMemcpyAsync(view.desc.as<char>(pl.defer_off), pl.defer_tasks.data(),
-                                   sizeof(int32_t) * pl.defer_tasks.size(), cudaMemcpyHostToDevice, s));
     FusedParams p = fused_params(&view, d_val_out, d_idx_out, idx_bytes, d_val_in, d_idx_in, k, flags);
     rc = run_fused(&view, p, flags, s);
     if (rc) return rc;

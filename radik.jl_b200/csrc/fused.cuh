@@ -39,8 +39,9 @@ namespace radik {
 // to its candidate region (no per-segment selection); the merge kernel
 // (merge.cuh) finishes it.
 // kTaskDefer: a single-segment task whose streaming block leaves its
-// candidates in the task's region (p.cap entries) for the merge kernel to
-// finish, so that the block moves on to its next task at once.
+// candidates in the task's region (p.cap entries) and queues it, so that the
+// block moves on to its next task at once; blocks with no streaming left
+// finish queued tasks (fused_ws.cuh).
 enum : uint32_t { kTaskLargest = 1u, kTaskAscend = 2u, kTaskSampled = 4u, kTaskFlush = 8u, kTaskDefer = 16u };
 
 struct FusedTask {
@@ -93,6 +94,9 @@ struct FusedParams {
     uint64_t* cand;          // candidate regions
     uint64_t* sort_scratch;  // [gridDim.x * kmax] (kmax > 4096 only)
     uint32_t* rank_ready;    // [T] merge kernel left the k output keys for rank_write_kernel (nullable)
+    uint32_t* defer_ctr;     // [2] deferred tasks queued / claimed by finishers
+    uint32_t* defer_q;       // [ndefer] queued task + 1 (0: not yet); nullable: no deferral
+    uint32_t ndefer;         // deferred tasks of the launch
     uint32_t* err;
 };
 

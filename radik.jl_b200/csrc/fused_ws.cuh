@@ -619,14 +619,22 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
 
             if (flush) {
                 // merge.cuh selects the task's k best from its candidate region.
-            } else if (!multi && (td.flags & kTaskDefer) != 0u && !p.retry) {
+            } else if (!multi && (td.flags & kTaskDefer) != 0u && !p.retry && p.defer_q != nullptr) {
                 // Deferred finish: the candidates (at least min(len, k), all in
-                // [0, sh.f.cnt) after the gather) to the task's region; the
-                // merge kernel selects, sorts and writes the row.
+                // [0, sh.f.cnt) after the gather) to the task's region, then the
+                // task into the ready queue; a block with no streaming left
+                // selects, sorts and writes the row (finisher loop below).
                 const uint32_t cnt = buffer_count<THREADS>(p, sh.f);
                 uint64_t* dst = p.cand + td.cbase;
                 for (uint32_t i = tid; i < cnt; i += THREADS) dst[i] = s_buf[i];
                 if (tid == 0) p.task_cnt[t] = cnt;
+                __threadfence();  // the region and the count before the publication
+                block_sync<THREADS>();
+                if (tid == 0) {
+                    const uint32_t j = atomicAdd(p.defer_ctr, 1u);
+                    if (j < p.ndefer) atomicExch(p.defer_q + j, static_cast<uint32_t>(t) + 1u);
+                    else record_error(p.err, kErrInternal);
+                }
             } else if (!multi) {
                 uint64_t kth = 0;
                 const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
@@ -712,6 +720,60 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
         }
         block_sync<THREADS>();  // the item is finished: its slot may be reused
         if (tid == 0) mbar_arrive(item_empty + slot);
+    }
+
+    // Finisher loop: no streaming work is left for this block; finish the
+    // deferred tasks that other blocks (or this one) queued, in queue order.
+    // Every queued slot is filled exactly once by the block that streamed
+    // the task, and all blocks of the grid are resident, so each wait ends;
+    // it is bounded all the same.
+    if (p.defer_q != nullptr && !p.retry) {
+        for (;;) {
+            if (tid == 0) {
+                int32_t job = -1;
+                if (!ld_volatile_u32(&sh.f.abort)) {
+                    const uint32_t j = atomicAdd(p.defer_ctr + 1, 1u);
+                    if (j < p.ndefer) job = static_cast<int32_t>(j);
+                }
+                uint32_t v = 0;
+                if (job >= 0) {
+                    for (uint32_t polls = 0; polls < kWaitPolls; ++polls) {
+                        v = ld_volatile_u32(p.defer_q + job);
+                        if (v != 0u) break;
+                        __nanosleep(64);
+                    }
+                    if (v == 0u) {
+                        record_error(p.err, kErrTimeout);
+                        st_volatile_u32(&sh.f.abort, 1u);
+                    }
+                }
+                sh.f.last = v;
+            }
+            block_sync<THREADS>();
+            const uint32_t v = sh.f.last;
+            block_sync<THREADS>();
+            if (v == 0u) break;
+            __threadfence();  // the region is read after its publication
+            const int t = static_cast<int>(v - 1u);
+            const FusedTask td = p.tasks[t];
+            const TaskView tv = task_view<kScale>(p, t, td);
+            const uint32_t k = tv.k;
+            uint32_t n = __ldcg(p.task_cnt + t);
+            if (n > p.cap) {  // never expected: the streaming block kept at most cap
+                if (tid == 0) record_error(p.err, kErrCapacity);
+                n = p.cap;
+            }
+            const unsigned long long* src = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
+#pragma unroll 4
+            for (uint32_t i = tid; i < n; i += THREADS) s_buf[i] = __ldcg(src + i);
+            if (tid == 0) sh.f.cnt = n;
+            block_sync<THREADS>();
+            uint64_t kth = 0;
+            const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
+            const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
+            if (m != want && tid == 0) record_error(p.err, kErrInternal);
+            finish_task<THREADS, !kScale>(p, tv, s_buf, m < want ? m : want, sh.f);
+        }
     }
 }
 

@@ -46,9 +46,7 @@ __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, cons
     const TaskView tv = task_view<kScale>(p, t, td);
     const uint32_t k = tv.k;
     const uint32_t cap = p.cap;
-    // A deferred task's region holds up to the streaming kernel's buffer (the
-    // launch passes that as p.cap); a flush-mode task's, nseg * kmax.
-    const uint32_t region = (td.flags & kTaskDefer) ? p.cap : static_cast<uint32_t>(td.nseg) * p.kmax;
+    const uint32_t region = static_cast<uint32_t>(td.nseg) * p.kmax;
     const uint32_t n = have < region ? have : region;
     const unsigned long long* src = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
     // Room kept free while streaming chunks: a shrink keeps at most mid_keep.
