@@ -100,10 +100,13 @@ __global__ void __launch_bounds__(THREADS) plain_select(PlainParams p, int pass,
         uint32_t rb = threadIdx.x * per + j;
         if (rb < nb) sum += gh[nb - 1 - rb];
     }
+    // Read the state before the scan: its barriers order every thread's reads
+    // before the one thread that owns rank r rewrites r and the bin below.
+    const uint32_t r = st->r;
+    const uint32_t ncand = st->ncand;
     uint32_t total;
     uint32_t before = block_exclusive_scan<THREADS>(sum, &total, s);
-    const uint32_t r = st->r;
-    if (threadIdx.x == 0 && total != st->ncand) record_error(p.err, kErrInternal);
+    if (threadIdx.x == 0 && total != ncand) record_error(p.err, kErrInternal);
     if (before < r && r <= before + sum) {
         uint32_t rr = r - before;
         for (uint32_t j = 0; j < per; ++j) {
