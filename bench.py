@@ -291,8 +291,10 @@ def run_ours(args, rank: int, world: int, dist):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     cfg = CONFIGS[args.config]
-    lens = task_lens_of(args.config)
-    T, k, N = len(lens), cfg["k"], int(sum(lens))
+    # Task lengths as an int64 array, as a caller that reuses a batch shape
+    # keeps them (a Python list is converted on every call).
+    lens = np.asarray(task_lens_of(args.config), dtype=np.int64)
+    T, k, N = len(lens), cfg["k"], int(lens.sum())
     # Inputs: enough rotating copies that the bytes touched between two reads
     # of the same buffer exceed the L2 several times.
     nbuf = max(2, int(np.ceil(3 * L2_BYTES / (4 * N))) + 1)

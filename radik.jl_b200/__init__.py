@@ -53,8 +53,12 @@ def _stream(stream) -> ctypes.c_void_p:
 
 
 def _lens_array(task_lens) -> np.ndarray:
-    a = np.ascontiguousarray(np.asarray(task_lens, dtype=np.int64).reshape(-1))
-    return a
+    """task_lens as a contiguous int64 array: free for such an array, a
+    conversion (tens of microseconds for a thousand tasks) for a list."""
+    if isinstance(task_lens, np.ndarray) and task_lens.dtype == np.int64 and task_lens.ndim == 1 \
+            and task_lens.flags.c_contiguous:
+        return task_lens
+    return np.ascontiguousarray(np.asarray(task_lens, dtype=np.int64).reshape(-1))
 
 
 def _check_cuda(t, what: str):

@@ -536,24 +536,33 @@ size_t plan_desc_bytes(const Plan& pl) { return pl.merge_off + sizeof(int32_t) *
 // Key of a call's plan: the batch shape and the configuration that applies
 // to it (one chosen by radik_ws_autotune for this shape, else the defaults),
 // with environment overrides on top.
+constexpr uint32_t kPlanFlags = RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN;
+
+// Whether a key describes this batch shape (its tuning aside); compares the
+// task lengths in place (no copy: calls with a thousand tasks repeat this).
+bool key_matches(const PlanKey& q, const int64_t* lens, int64_t T, int64_t k, uint32_t mflags, int idx_bytes) {
+    return q.k == k && q.flags == mflags && q.idx_bytes == idx_bytes && static_cast<int64_t>(q.lens.size()) == T &&
+           std::equal(q.lens.begin(), q.lens.end(), lens);
+}
+
+// The configuration for a batch shape: the one radik_ws_autotune chose for
+// it, else the defaults; environment overrides on top.
+TuneConfig shape_config(const radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t mflags,
+                        int idx_bytes) {
+    TuneConfig tc;
+    for (const auto& e : ws->tuned)
+        if (key_matches(e.first, lens, T, k, mflags, idx_bytes)) { tc = e.second; break; }
+    return with_env(tc);
+}
+
 PlanKey plan_key(const radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes,
                  const TuneConfig* force = nullptr) {
     PlanKey key;
     key.lens.assign(lens, lens + T);
     key.k = k;
-    key.flags = flags & (RADIK_LARGEST | RADIK_ASCEND | RADIK_WITHSCALE | RADIK_WITHIDXIN | RADIK_PLAIN);
+    key.flags = flags & kPlanFlags;
     key.idx_bytes = idx_bytes;
-    TuneConfig tc;
-    if (force) {
-        tc = *force;
-    } else {
-        for (const auto& e : ws->tuned) {
-            PlanKey kk = key;
-            kk.tune = e.first.tune;
-            if (e.first == kk) { tc = e.second; break; }
-        }
-    }
-    key.tune = with_env(tc);
+    key.tune = force ? with_env(*force) : shape_config(ws, lens, T, k, key.flags, idx_bytes);
     return key;
 }
 
@@ -563,8 +572,14 @@ PlanKey plan_key(const radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, 
 int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t flags, int idx_bytes,
                cudaStream_t upload = nullptr, bool use_upload = false) {
     Plan& pl = ws->plan;
+    {
+        // The plan of the last call usually fits: check it without building a key.
+        const uint32_t mflags = flags & kPlanFlags;
+        if (pl.valid && key_matches(pl.key, lens, T, k, mflags, idx_bytes) &&
+            pl.key.tune == shape_config(ws, lens, T, k, mflags, idx_bytes))
+            return RADIK_OK;
+    }
     PlanKey key = plan_key(ws, lens, T, k, flags, idx_bytes);
-    if (pl.valid && pl.key == key) return RADIK_OK;
 
     Plan np;
     np.key = key;
@@ -972,8 +987,10 @@ int radik_topk_radix_select(float* d_val_out, void* d_idx_out, int idx_bytes, ra
         ((flags & RADIK_WITHIDXIN) && (reinterpret_cast<uintptr_t>(d_idx_in) & (idx_bytes - 1))))
         return fail(RADIK_ERR_INVALID, "device arrays must be aligned to their element size");
     {
-        const PlanKey key = plan_key(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
-        if (!(ws->plan.valid && ws->plan.key == key)) {
+        const uint32_t mflags = flags & kPlanFlags;
+        const bool have_plan = ws->plan.valid && key_matches(ws->plan.key, h_task_lens, num_tasks, k, mflags, idx_bytes) &&
+                               ws->plan.key.tune == shape_config(ws, h_task_lens, num_tasks, k, mflags, idx_bytes);
+        if (!have_plan) {
             if (cap != cudaStreamCaptureStatusNone)
                 return fail(RADIK_ERR_CAPTURE, "no prepared plan for this shape: call radik_ws_prepare before capture");
             rc = build_plan(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
