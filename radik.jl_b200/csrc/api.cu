@@ -8,6 +8,7 @@
 #include <mutex>
 #include <numeric>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/radik.h"
@@ -699,6 +700,26 @@ FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, c
     return p;
 }
 
+// Launch of a kernel that follows another kernel on the stream: with
+// programmatic stream serialization the launch overlaps the end of the
+// previous kernel (the kernel waits in grid_dep_wait before reading its
+// results).  `after_kernel` false: an ordinary launch.
+template <typename... KArgs, typename... AArgs>
+cudaError_t launch_after(bool after_kernel, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                         cudaStream_t s, AArgs&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = after_kernel ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<AArgs>(args)...);
+}
+
 int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s) {
     const Plan& pl = ws->plan;
     const StateLayout L(pl.T);
@@ -714,21 +735,20 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
     }
     FusedKernel fk = pl.ws_form ? pick_fused_ws(pl.threads, pl.vec, pl.ws_stages, scale)
                                 : pick_fused(pl.threads, pl.vec, scale);
-    fk<<<pl.grid, pl.launch_threads, pl.smem, s>>>(p);
-    RADIK_CUDA(cudaGetLastError());
+    RADIK_CUDA(launch_after(!pl.jobs.empty(), fk, dim3(pl.grid), dim3(pl.launch_threads), pl.smem, s, p));
     if (!pl.merge_tasks.empty()) {
         // Flush-mode tasks: exact selection from their candidate regions.
         FusedParams m = p;
         m.cap = pl.merge_cap;
-        pick_merge(scale)<<<static_cast<unsigned>(pl.merge_tasks.size()), kMergeThreads, pl.merge_smem, s>>>(
-            m, ws->desc.as<int32_t>(pl.merge_off));
-        RADIK_CUDA(cudaGetLastError());
+        RADIK_CUDA(launch_after(true, pick_merge(scale), dim3(static_cast<unsigned>(pl.merge_tasks.size())),
+                                dim3(kMergeThreads), pl.merge_smem, s, m,
+                                static_cast<const int32_t*>(ws->desc.as<int32_t>(pl.merge_off))));
         // ... and the output rows of those it left to the rank kernel.
         const dim3 rgrid(static_cast<unsigned>((p.kmax + kRankPerBlock - 1) / kRankPerBlock),
                          static_cast<unsigned>(pl.merge_tasks.size()));
         const size_t rsmem = sizeof(uint64_t) * (std::min<size_t>(p.kmax, kRankMaxK) + 2);
-        pick_rank(scale)<<<rgrid, kRankThreads, rsmem, s>>>(m, ws->desc.as<int32_t>(pl.merge_off));
-        RADIK_CUDA(cudaGetLastError());
+        RADIK_CUDA(launch_after(true, pick_rank(scale), rgrid, dim3(kRankThreads), rsmem, s, m,
+                                static_cast<const int32_t*>(ws->desc.as<int32_t>(pl.merge_off))));
     }
     if (!pl.jobs.empty()) {
         // Recompute, without the sampled threshold and with the full candidate
@@ -742,8 +762,7 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
         r.task_done = ws->state.as<uint32_t>(L.done_r);
         r.task_cnt = ws->state.as<uint32_t>(L.cnt_r);
         FusedKernel rk = pick_fused(pl.retry_threads, pl.retry_vec, scale);
-        rk<<<pl.retry_grid, pl.retry_threads, pl.retry_smem, s>>>(r);
-        RADIK_CUDA(cudaGetLastError());
+        RADIK_CUDA(launch_after(true, rk, dim3(pl.retry_grid), dim3(pl.retry_threads), pl.retry_smem, s, r));
     }
     return RADIK_OK;
 }

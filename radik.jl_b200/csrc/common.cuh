@@ -165,6 +165,12 @@ __device__ __forceinline__ bool block_sync_or(bool pred) {
     return r != 0;
 }
 
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream serialization attribute may start while the previous kernel of its
+// stream finishes; it waits here before it reads anything that kernel wrote.
+// Without the attribute this returns at once.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void record_error(uint32_t* err, uint32_t bits) {
     if (err) atomicOr(err, bits);
 }

@@ -483,6 +483,7 @@ __device__ __forceinline__ void issue_prologue(float* ring, uint64_t* bars, cons
 
 template <int THREADS, int VEC, int STAGES, bool kScale>
 __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_kernel(FusedParams p) {
+    grid_dep_wait();  // launched after the previous kernel of the call
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ FusedShared<THREADS> sh;
     constexpr int U = VEC / 4;                      // float4 per thread per tile

@@ -32,6 +32,7 @@ constexpr int kRankPerBlock = kRankThreads / kRankSplit;  // output keys placed 
 
 template <int THREADS, bool kScale>
 __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, const int32_t* merge_tasks) {
+    grid_dep_wait();  // launched after the streaming kernel
     extern __shared__ __align__(16) uint64_t s_buf[];
     __shared__ FusedShared<THREADS> sh;
     __shared__ uint32_t s_spill_n;        // block_topk_bound_regs: entries of the boundary bin
@@ -147,6 +148,7 @@ __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, cons
 // writes the value and index there.
 template <bool kScale>
 __global__ void __launch_bounds__(kRankThreads) rank_write_kernel(FusedParams p, const int32_t* merge_tasks) {
+    grid_dep_wait();  // launched after the merge kernel
     extern __shared__ __align__(16) uint64_t s_keys[];
     const int tid = threadIdx.x;
     const int t = merge_tasks[blockIdx.y];
