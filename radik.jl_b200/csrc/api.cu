@@ -700,6 +700,12 @@ FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, c
     return p;
 }
 
+// Clears the per-call state (n 32-bit words): a kernel rather than a memset,
+// so that the call's first kernel can be launched programmatically after it.
+__global__ void state_clear_kernel(uint32_t* p, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0u;
+}
+
 // Launch of a kernel that follows another kernel on the stream: with
 // programmatic stream serialization the launch overlaps the end of the
 // previous kernel (the kernel waits in grid_dep_wait before reading its
@@ -725,17 +731,22 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
     const StateLayout L(pl.T);
     const bool scale = (flags & RADIK_WITHSCALE) != 0;
     // Reset the per-call state (the error word stays sticky until read).
-    RADIK_CUDA(cudaMemsetAsync(ws->state.as<char>(StateLayout::kWork), 0, L.bytes - StateLayout::kWork, s));
+    {
+        const uint32_t nw = static_cast<uint32_t>((L.bytes - StateLayout::kWork) / 4);
+        const unsigned cg = std::max(1u, std::min(148u * 4u, (nw + 255u) / 256u));
+        state_clear_kernel<<<cg, 256, 0, s>>>(ws->state.as<uint32_t>(StateLayout::kWork), nw);
+        RADIK_CUDA(cudaGetLastError());
+    }
     if (!pl.jobs.empty()) {
         SampleKernel sk = pick_sample(scale);
         const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
-        sk<<<static_cast<unsigned>(pl.jobs.size()), 256, ssmem, s>>>(
-            p, ws->desc.as<SampleJob>(pl.jobs_off), ws->samples.as<uint64_t>(), ws->state.as<uint32_t>(L.sdone));
-        RADIK_CUDA(cudaGetLastError());
+        RADIK_CUDA(launch_after(true, sk, dim3(static_cast<unsigned>(pl.jobs.size())), dim3(256), ssmem, s, p,
+                                static_cast<const SampleJob*>(ws->desc.as<SampleJob>(pl.jobs_off)),
+                                ws->samples.as<uint64_t>(), ws->state.as<uint32_t>(L.sdone)));
     }
     FusedKernel fk = pl.ws_form ? pick_fused_ws(pl.threads, pl.vec, pl.ws_stages, scale)
                                 : pick_fused(pl.threads, pl.vec, scale);
-    RADIK_CUDA(launch_after(!pl.jobs.empty(), fk, dim3(pl.grid), dim3(pl.launch_threads), pl.smem, s, p));
+    RADIK_CUDA(launch_after(true, fk, dim3(pl.grid), dim3(pl.launch_threads), pl.smem, s, p));
     if (!pl.merge_tasks.empty()) {
         // Flush-mode tasks: exact selection from their candidate regions.
         FusedParams m = p;
@@ -964,7 +975,8 @@ int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
     // fused: sampling kernel + fused kernel (+ merge kernel for flush-mode
     // tasks) + retry launch when sampled;
     // multi-pass: histogram, select, compact, advance, finalize at least.
-    info->kernels_per_call = pl.fused ? 1 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) : 5;
+    // state clear + streaming kernel (+ sampler and retry) (+ merge and rank)
+    info->kernels_per_call = pl.fused ? 2 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) : 5;
     return RADIK_OK;
 }
 

@@ -298,7 +298,7 @@ __device__ __forceinline__ uint32_t ws_place(const float4* src, uint32_t elems, 
 
 template <int NCW, int J, int STAGES, bool kScale>
 __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_kernel(FusedParams p) {
-    grid_dep_wait();  // launched after the previous kernel of the call (the sampler)
+    grid_dep_wait();  // launched after the previous kernel of the call (state clear or sampler)
     constexpr int THREADS = NCW * 32;             // consumer threads
     constexpr uint32_t TW = 128u * J;             // elements per warp tile (one ring stage)
     constexpr uint32_t TW4 = TW / 4;              // float4 per warp tile

@@ -37,6 +37,7 @@ struct SampleJob {
 template <int THREADS, bool kScale>
 __global__ void __launch_bounds__(THREADS) sample_threshold_kernel(FusedParams p, const SampleJob* jobs,
                                                                     uint64_t* sample_out, uint32_t* sample_done) {
+    grid_dep_wait();  // launched after the state is cleared
     extern __shared__ __align__(16) uint64_t s_buf[];
     __shared__ FusedShared<THREADS> sh;
     constexpr uint32_t kChunk4 = kSampleChunk / 4;  // float4 per chunk
