@@ -700,6 +700,15 @@ FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, c
     return p;
 }
 
+// The rank kernel places every output key by counting the keys below it:
+// k^2 compares per task, spread over the GPU.  That pays off for a few tasks
+// (one large task's merge runs on one SM otherwise); for many flush-mode
+// tasks their merge blocks already fill the GPU and sort their rows
+// themselves.
+bool rank_pays(size_t ntasks, uint64_t k) {
+    return k <= kRankMaxK && static_cast<uint64_t>(ntasks) * k * k <= (uint64_t(1) << 26);
+}
+
 // Clears the per-call state (n 32-bit words): a kernel rather than a memset,
 // so that the call's first kernel can be launched programmatically after it.
 __global__ void state_clear_kernel(uint32_t* p, uint32_t n) {
@@ -751,15 +760,19 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
         // Flush-mode tasks: exact selection from their candidate regions.
         FusedParams m = p;
         m.cap = pl.merge_cap;
+        const bool use_rank = rank_pays(pl.merge_tasks.size(), p.kmax);
+        if (!use_rank) m.rank_ready = nullptr;  // each merge block sorts and writes its row
         RADIK_CUDA(launch_after(true, pick_merge(scale), dim3(static_cast<unsigned>(pl.merge_tasks.size())),
                                 dim3(kMergeThreads), pl.merge_smem, s, m,
                                 static_cast<const int32_t*>(ws->desc.as<int32_t>(pl.merge_off))));
         // ... and the output rows of those it left to the rank kernel.
-        const dim3 rgrid(static_cast<unsigned>((p.kmax + kRankPerBlock - 1) / kRankPerBlock),
-                         static_cast<unsigned>(pl.merge_tasks.size()));
-        const size_t rsmem = sizeof(uint64_t) * (std::min<size_t>(p.kmax, kRankMaxK) + 2);
-        RADIK_CUDA(launch_after(true, pick_rank(scale), rgrid, dim3(kRankThreads), rsmem, s, m,
-                                static_cast<const int32_t*>(ws->desc.as<int32_t>(pl.merge_off))));
+        if (use_rank) {
+            const dim3 rgrid(static_cast<unsigned>((p.kmax + kRankPerBlock - 1) / kRankPerBlock),
+                             static_cast<unsigned>(pl.merge_tasks.size()));
+            const size_t rsmem = sizeof(uint64_t) * (std::min<size_t>(p.kmax, kRankMaxK) + 2);
+            RADIK_CUDA(launch_after(true, pick_rank(scale), rgrid, dim3(kRankThreads), rsmem, s, m,
+                                    static_cast<const int32_t*>(ws->desc.as<int32_t>(pl.merge_off))));
+        }
     }
     if (!pl.jobs.empty()) {
         // Recompute, without the sampled threshold and with the full candidate
@@ -976,7 +989,10 @@ int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
     // tasks) + retry launch when sampled;
     // multi-pass: histogram, select, compact, advance, finalize at least.
     // state clear + streaming kernel (+ sampler and retry) (+ merge and rank)
-    info->kernels_per_call = pl.fused ? 2 + (pl.jobs.empty() ? 0 : 2) + (pl.merge_tasks.empty() ? 0 : 2) : 5;
+    info->kernels_per_call =
+        pl.fused ? 2 + (pl.jobs.empty() ? 0 : 2) +
+                       (pl.merge_tasks.empty() ? 0 : (rank_pays(pl.merge_tasks.size(), pl.key.k) ? 2 : 1))
+                 : 5;
     return RADIK_OK;
 }
 

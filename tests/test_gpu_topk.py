@@ -315,3 +315,26 @@ def test_deferred_finish(oracle, radik, torch_cuda, monkeypatch, k):
     ind = rng.permutation(sum(lens)).astype(np.int64) * 3 + 1
     _compare(oracle, radik, torch_cuda, x, lens, k, indices=ind)
     _compare(oracle, radik, torch_cuda, x + 5.0, lens, k, withscale=True)
+
+
+def test_multipass_repeated_calls_stay_consistent(oracle, radik, torch_cuda):
+    """The multi-pass path on a batch of many tasks, called repeatedly with
+    one workspace: every call must leave the device error word clear (its
+    rank search once let a slow warp read a residual rank that another
+    thread had already updated) and match the oracle."""
+    rng = np.random.default_rng(41)
+    lens = [int(v) for v in np.clip(rng.lognormal(np.log(20000), 1.5, size=2048), 1, 400_000)]
+    x = rng.standard_normal(sum(lens)).astype(np.float32)
+    dev = torch_cuda.device("cuda")
+    xt = torch_cuda.from_numpy(x).to(dev)
+    T, k = len(lens), 64
+    vo = torch_cuda.empty((T, k), dtype=torch_cuda.float32, device=dev)
+    io = torch_cuda.empty((T, k), dtype=torch_cuda.int32, device=dev)
+    ws = radik.RadiKWorkspace("cuda", max(lens), T)
+    ov, oi = oracle.topk(x, lens, k)
+    for _ in range(12):
+        radik.topk_radix_select_(vo, io, ws, xt, None, lens, k, True, True, plain=True)
+        assert ws.error_bits() == 0
+        assert np.array_equal(vo.cpu().numpy().view(np.uint32), ov.view(np.uint32))
+        assert np.array_equal(io.cpu().numpy().astype(np.int64), oi.astype(np.int64))
+    ws.close()
