@@ -493,7 +493,7 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
         std::vector<int32_t> elig;
         for (int64_t t = 0; t < T; ++t) {
             const FusedTask& td = np.tasks[t];
-            if (td.nseg == 1 && td.len > static_cast<int64_t>(kk) && td.len >= 16384 && (td.flags & kTaskSampled) == 0)
+            if (td.nseg == 1 && td.len > static_cast<int64_t>(kk) && td.len >= 4096 && (td.flags & kTaskSampled) == 0)
                 elig.push_back(static_cast<int32_t>(t));
         }
         const bool want = tc.defer > 0 || static_cast<int64_t>(elig.size()) >= resident;

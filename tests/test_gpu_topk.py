@@ -304,7 +304,7 @@ def test_deferred_finish(oracle, radik, torch_cuda, monkeypatch, k):
     monkeypatch.setenv("RADIK_DEFER", "1")
     monkeypatch.setenv("RADIK_WS", "1")
     rng = np.random.default_rng(500 + k)
-    lens = [65536] * 24 + [16384, 40000, 100, 0, 3, 200_000, 70_001]
+    lens = [65536] * 24 + [16384, 40000, 100, 0, 3, 200_000, 70_001, 4096, 5003]
     x = rng.standard_normal(sum(lens)).astype(np.float32)
     _compare(oracle, radik, torch_cuda, x, lens, k)
     _compare(oracle, radik, torch_cuda, x, lens, k, largest=False, rev=True)
