@@ -4,15 +4,16 @@
 // all its elements above the task's seeded threshold to the task's candidate
 // region: a superset of the task's k best.  One block per such task selects
 // the exact k best of the region:
-//   * usual case (the region fits in shared memory beside the scratch below,
-//     k <= kRankMaxK): the region is loaded at once and the k-th largest
-//     composite is found with 8-bit digit windows (per-warp histograms) that
-//     narrow it to one bin, whose entries one warp then bisects; the k
-//     selected entries are written back to the region as output sort keys,
-//     and rank_write_kernel
-//     puts every one at its place in the output row: its place is the number
-//     of the k keys below it, counted by many blocks at once (k^2 compares
-//     spread over the GPU instead of a sorting network on one SM);
+//   * when the launch passes rank_ready (few tasks: the host's rank_pays),
+//     the region fits in shared memory beside the select's scratch and
+//     k <= kRankMaxK: the region is loaded at once and the k-th largest
+//     composite is found with block_topk_bound (8-bit digit windows over
+//     per-warp histograms narrow it to one bin, whose entries one warp then
+//     bisects); the k selected entries are written back to the region as
+//     output sort keys, and rank_write_kernel puts every one at its place in
+//     the output row: its place is the number of the k keys below it,
+//     counted by many blocks at once (k^2 compares spread over the GPU
+//     instead of a sorting network on one SM);
 //   * otherwise the region is loaded into shared memory (in chunks, keeping a
 //     few more than k with block_shrink whenever the buffer fills), selected
 //     with block_select_topk, sorted and written by this block.
@@ -35,7 +36,7 @@ __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, cons
     grid_dep_wait();  // launched after the streaming kernel
     extern __shared__ __align__(16) uint64_t s_buf[];
     __shared__ FusedShared<THREADS> sh;
-    __shared__ uint32_t s_spill_n;        // block_topk_bound_regs: entries of the boundary bin
+    __shared__ uint32_t s_spill_n;        // block_topk_bound: entries of the boundary bin
     __shared__ unsigned long long s_tau;  // ... and the bound warp 0 found
     const int tid = threadIdx.x;
     const int t = merge_tasks[blockIdx.x];
