@@ -108,3 +108,16 @@ def test_uneven_batch_full_size(oracle, radik, torch_cuda):
     del x
     ov, oi = oracle.topk(x_np, lens, 64, largest=True, rev=False, indices=ind_np, idx_dtype=np.int32)
     _compare(oracle, vo, io, ov, oi)
+
+
+def test_adversarial_single_full_size_largest(oracle, radik, torch_cuda):
+    """The adversarial task's stress variant: the k largest (ascending),
+    where 40 % of the elements crowd one narrow band just above 1.0."""
+    bench = _bench()
+    n = 1 << 28
+    x_np = bench.make_input_np("adversarial_single", n)
+    x, vo, io = _run(radik, torch_cuda, x_np, [n], 4096, True, False)
+    _properties(torch_cuda, x, [n], vo, io, 4096, True, False)
+    del x
+    ov, oi = oracle.topk(x_np, [n], 4096, largest=True, rev=False)
+    _compare(oracle, vo, io, ov, oi)
