@@ -65,6 +65,8 @@ CONFIGS = {
     "uniform_batch": dict(k=256, largest=True, rev=False, custom_idx=False),
     "adversarial_single": dict(k=4096, largest=False, rev=True, custom_idx=False),
     "uneven_batch": dict(k=64, largest=True, rev=False, custom_idx=True),
+    # The reference's CPU-runnable case: one task of 2^20 N(0,1), seed 0.
+    "single_1m": dict(k=100, largest=True, rev=False, custom_idx=False),
 }
 
 
@@ -73,6 +75,8 @@ def task_lens_of(name: str) -> list[int]:
         return [65536] * 1024
     if name == "adversarial_single":
         return [1 << 28]
+    if name == "single_1m":
+        return [1 << 20]
     rng = np.random.default_rng(3)
     v = np.clip(np.round(rng.lognormal(np.log(20000), 1.5, size=4096)), 1, 4_194_304)
     return [int(x) for x in v]
@@ -93,6 +97,8 @@ def make_input_np(name: str, N: int, seed_offset: int = 0) -> np.ndarray:
         out[b] = (1.0 + rng.random(int(b.sum()), dtype=np.float32) * np.float32(2.0 ** -10)).astype(np.float32)
         out[c] = (rng.standard_normal(int(c.sum())).astype(np.float32) * np.float32(100.0))
         return out
+    if name == "single_1m":
+        return np.random.default_rng(seed_offset).standard_normal(N).astype(np.float32)
     return np.random.default_rng(3 + seed_offset).standard_normal(N).astype(np.float32)
 
 
@@ -205,6 +211,9 @@ def run_reference(args, rank: int, world: int):
     elif args.config == "adversarial_single":
         sample_lens = [1 << 22]
         sample = "a 2^22-element prefix task of the same mixture per step"
+    elif args.config == "single_1m":
+        sample_lens = lens
+        sample = "the whole 2^20-element task per step"
     else:
         sample_lens = lens[:256]
         sample = "the first 256 of the 4096 tasks per step"
@@ -272,6 +281,8 @@ def cpu_baseline_quick(args) -> dict:
         sl, sample = lens[:64], "64 of the 1024 tasks, 3 repetitions"
     elif args.config == "adversarial_single":
         sl, sample = [1 << 22], "one 2^22-element task of the same mixture, 3 repetitions"
+    elif args.config == "single_1m":
+        sl, sample = lens, "the whole 2^20-element task, 3 repetitions"
     else:
         sl, sample = lens[:256], "first 256 of the 4096 tasks, 3 repetitions"
     N = int(sum(sl))
@@ -282,7 +293,34 @@ def cpu_baseline_quick(args) -> dict:
     for _ in range(3):
         oracle.topk(x, sl, cfg["k"], largest=cfg["largest"], rev=cfg["rev"], threads=threads)
     dt = (time.perf_counter() - t0) / 3
-    return {"value": N / dt, "unit": "elements/s", "cores": threads, "kind": "port", "sample": sample}
+    return {"value": N / dt, "unit": "elements/s", "cores": threads, "kind": "port", "sample": sample,
+            "select_sort": select_sort_baseline(x, sl, cfg["k"], cfg["largest"])}
+
+
+def select_sort_baseline(x: np.ndarray, lens, k: int, largest: bool) -> dict:
+    """A generic CPU top-k for scale: per task an introselect partition
+    (numpy argpartition, the algorithm of std::nth_element) and a sort of the
+    k selected, one thread.  Its ties at the k-th value are not the lowest
+    positions, so it is a speed reference only, not a result to compare."""
+    def once():
+        a = 0
+        for n in lens:
+            n = int(n)
+            v = x[a:a + n]
+            kk = min(k, n)
+            if kk < n:
+                sel = np.argpartition(v, n - kk)[n - kk:] if largest else np.argpartition(v, kk - 1)[:kk]
+            else:
+                sel = np.arange(n)
+            sel[np.argsort(v[sel], kind="stable")]
+            a += n
+    once()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        once()
+    dt = (time.perf_counter() - t0) / 3
+    return {"value": int(sum(lens)) / dt, "unit": "elements/s", "cores": 1,
+            "method": "numpy argpartition (introselect) + sort of the k, per task"}
 
 
 def run_ours(args, rank: int, world: int, dist):
