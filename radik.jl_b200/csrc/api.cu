@@ -144,7 +144,7 @@ int env_int(const char* name, int dflt) {
 // Tunable shape of a plan.  Defaults are the measured best for the common
 // cases; radik_ws_autotune picks another per batch shape; environment
 // variables (RADIK_WS, RADIK_WST, RADIK_WSJ, RADIK_WSS, RADIK_WS_SAMPLE,
-// RADIK_WS_WINDOWS, RADIK_SEG_DIV, RADIK_DEFER) override both, for
+// RADIK_WS_WINDOWS, RADIK_SEG_DIV, RADIK_DEFER, RADIK_SEG_MIN) override both, for
 // experiments.
 struct TuneConfig {
     int form = -1;          // -1 automatic, 0 barrier form, 1 warp-specialised form
@@ -155,10 +155,11 @@ struct TuneConfig {
     int sample_windows = 2; // digit windows of its rank threshold
     int seg_div = 3;        // work items per resident block when splitting tasks
     int defer = -1;         // deferred finish of single-segment tasks: -1 automatic, 0 no, 1 yes
+    int seg_min_tiles = 64; // shortest segment of a split task, in 2048-element tiles
     bool operator==(const TuneConfig& o) const {
         return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
                sample_max == o.sample_max && sample_windows == o.sample_windows && seg_div == o.seg_div &&
-               defer == o.defer;
+               defer == o.defer && seg_min_tiles == o.seg_min_tiles;
     }
 };
 
@@ -171,6 +172,7 @@ TuneConfig with_env(TuneConfig c) {
     c.sample_windows = env_int("RADIK_WS_WINDOWS", c.sample_windows);
     c.seg_div = std::max(1, env_int("RADIK_SEG_DIV", c.seg_div));
     c.defer = env_int("RADIK_DEFER", c.defer);
+    c.seg_min_tiles = std::max(1, env_int("RADIK_SEG_MIN", c.seg_min_tiles));
     if (c.sample_max != 2048 && c.sample_max != 4096) c.sample_max = 2048;
     return c;
 }
@@ -289,13 +291,15 @@ size_t fused_cap(size_t k, size_t tile, int threads) {
     return round_up(cap, 64);
 }
 
-// Segment length: about three work items per resident block, at least 64
-// tiles, a multiple of the tile (env RADIK_SEG overrides).
-int64_t pick_seg_len(int64_t N, int64_t resident, size_t tile, bool fused, int seg_div) {
+// Segment length: about seg_div work items per resident block, at least
+// min_tiles tiles (64 by default; a short single task runs faster on more,
+// smaller, sampled segments), a multiple of the tile (env RADIK_SEG
+// overrides).
+int64_t pick_seg_len(int64_t N, int64_t resident, size_t tile, bool fused, int seg_div, int min_tiles) {
     int64_t seg_len = env_int("RADIK_SEG", 0);
     if (seg_len <= 0) {
         const int64_t target = N / std::max<int64_t>(1, seg_div * resident);
-        seg_len = std::max<int64_t>(64 * static_cast<int64_t>(tile), target);
+        seg_len = std::max<int64_t>(static_cast<int64_t>(min_tiles) * static_cast<int64_t>(tile), target);
     }
     seg_len = static_cast<int64_t>(round_up(static_cast<size_t>(seg_len), tile));
     if (!fused) seg_len = std::max<int64_t>(seg_len, 1 << 20);
@@ -420,7 +424,8 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
 
     // Segments and samples first, sized for the warp-specialised form's
     // residency (four blocks per SM).
-    segment_tasks(np, lens, T, k, flags, pick_seg_len(np.N, 4LL * di.sms, seg_tile, !plain, tc.seg_div), !plain);
+    segment_tasks(np, lens, T, k, flags,
+                  pick_seg_len(np.N, 4LL * di.sms, seg_tile, !plain, tc.seg_div, tc.seg_min_tiles), !plain);
     bool all_flush = T > 0;  // every non-empty task is split and sampled
     for (int64_t t = 0; t < T; ++t)
         if (lens[t] > 0 && (np.tasks[t].flags & kTaskSampled) == 0) all_flush = false;
@@ -474,7 +479,9 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
         // Re-segment for the form that runs.
         occ = std::max(occ, 1);
         segment_tasks(np, lens, T, k, flags,
-                      pick_seg_len(np.N, static_cast<int64_t>(occ) * di.sms, seg_tile, np.fused, tc.seg_div), np.fused);
+                      pick_seg_len(np.N, static_cast<int64_t>(occ) * di.sms, seg_tile, np.fused, tc.seg_div,
+                                   tc.seg_min_tiles),
+                      np.fused);
     }
     const int64_t resident = static_cast<int64_t>(occ) * di.sms;
     np.merge_tasks.clear();
@@ -1069,8 +1076,9 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     if (capst != cudaStreamCaptureStatusNone) return fail(RADIK_ERR_CAPTURE, "autotuning cannot run during capture");
     reps = std::max(1, std::min(reps, 100));
     // Candidate shapes: the defaults, other rings and block sizes of the
-    // warp-specialised form, a larger sample, the barrier form, and other
-    // segment sizes for split tasks.
+    // warp-specialised form, a larger sample, the barrier form, other
+    // segment sizes for split tasks, and short segments (4 tiles), which
+    // spread a single task of a few million elements over the whole GPU.
     std::vector<TuneConfig> cands;
     TuneConfig d;
     cands.push_back(d);
@@ -1082,6 +1090,7 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     { TuneConfig c = d; c.seg_div = 6; cands.push_back(c); }
     { TuneConfig c = d; c.defer = 0; cands.push_back(c); }
     { TuneConfig c = d; c.defer = 1; cands.push_back(c); }
+    { TuneConfig c = d; c.seg_min_tiles = 4; cands.push_back(c); }
     PlanKey base = plan_key(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
     auto set_choice = [&](const TuneConfig& c) {
         for (auto& e : ws->tuned) {

@@ -317,6 +317,35 @@ def test_deferred_finish(oracle, radik, torch_cuda, monkeypatch, k):
     _compare(oracle, radik, torch_cuda, x + 5.0, lens, k, withscale=True)
 
 
+@pytest.mark.parametrize("k", [1, 100, 1000, 4096])
+def test_short_segments_single_task(oracle, radik, torch_cuda, monkeypatch, k):
+    """The autotuner's short-segment plan (RADIK_SEG_MIN=4: 8192-element
+    segments) on the 2^20-element N(0,1) task of seed 0: 128 segments, with a
+    sampled threshold and the merge kernel where the segments' candidates
+    would be many (128 k >= 8192) and the sample's rank allows it (k <= 1000
+    here), else unsampled with every segment's k candidates."""
+    monkeypatch.setenv("RADIK_SEG_MIN", "4")
+    n = 1 << 20
+    x = np.random.default_rng(0).standard_normal(n).astype(np.float32)
+    ws = radik.RadiKWorkspace("cuda", n, 1)
+    ws.prepare([n], k)
+    info = ws.plan_info()
+    ws.close()
+    assert info["segments"] == 128
+    assert (info["sample_jobs"] > 0) == (64 <= k <= 1000)
+    _compare(oracle, radik, torch_cuda, x, [n], k)
+    _compare(oracle, radik, torch_cuda, x, [n], k, largest=False, rev=True)
+    q = np.round(x * 32.0).astype(np.float32) / 32.0  # ties at the k-th value
+    q[::1013] = np.nan
+    _compare(oracle, radik, torch_cuda, q, [n], k, rev=True)
+    _compare(oracle, radik, torch_cuda, x + 3.0, [n], k, withscale=True)
+    # a batch of a few such tasks beside short ones
+    lens = [n, 3 * n // 2, 20_000, 7]
+    y = np.random.default_rng(k + 1).standard_normal(sum(lens)).astype(np.float32)
+    ind = np.random.default_rng(k + 2).permutation(sum(lens)).astype(np.int32)
+    _compare(oracle, radik, torch_cuda, y, lens, k, indices=ind)
+
+
 def test_multipass_repeated_calls_stay_consistent(oracle, radik, torch_cuda):
     """The multi-pass path on a batch of many tasks, called repeatedly with
     one workspace: every call must leave the device error word clear (its
