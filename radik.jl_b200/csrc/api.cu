@@ -155,7 +155,7 @@ struct TuneConfig {
     int sample_windows = 2; // digit windows of its rank threshold
     int seg_div = 3;        // work items per resident block when splitting tasks
     int defer = -1;         // deferred finish of single-segment tasks: -1 automatic, 0 no, 1 yes
-    int seg_min_tiles = 64; // shortest segment of a split task, in 2048-element tiles
+    int seg_min_tiles = 0;  // shortest segment of a split task in 2048-element tiles; 0 automatic
     bool operator==(const TuneConfig& o) const {
         return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
                sample_max == o.sample_max && sample_windows == o.sample_windows && seg_div == o.seg_div &&
@@ -172,7 +172,7 @@ TuneConfig with_env(TuneConfig c) {
     c.sample_windows = env_int("RADIK_WS_WINDOWS", c.sample_windows);
     c.seg_div = std::max(1, env_int("RADIK_SEG_DIV", c.seg_div));
     c.defer = env_int("RADIK_DEFER", c.defer);
-    c.seg_min_tiles = std::max(1, env_int("RADIK_SEG_MIN", c.seg_min_tiles));
+    c.seg_min_tiles = std::max(0, env_int("RADIK_SEG_MIN", c.seg_min_tiles));
     if (c.sample_max != 2048 && c.sample_max != 4096) c.sample_max = 2048;
     return c;
 }
@@ -421,11 +421,18 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     np.ws_sample_max = tc.sample_max;
     np.ws_sample_windows = tc.sample_windows;
     const size_t seg_tile = 2048;  // segments are whole tiles of either form
+    // Shortest segment.  A single task too short to give every SM a 64-tile
+    // segment is cut into 4-tile segments, sampled, and merged: 2^20 to 2^24
+    // elements ran up to 2x faster that way (k up to 1024; a larger k would
+    // leave short segments unsampled, every element a candidate).
+    const int min_tiles =
+        tc.seg_min_tiles > 0 ? tc.seg_min_tiles
+                             : ((T == 1 && k <= 1024 && np.N < static_cast<int64_t>(di.sms) * 64 * seg_tile) ? 4 : 64);
 
     // Segments and samples first, sized for the warp-specialised form's
     // residency (four blocks per SM).
-    segment_tasks(np, lens, T, k, flags,
-                  pick_seg_len(np.N, 4LL * di.sms, seg_tile, !plain, tc.seg_div, tc.seg_min_tiles), !plain);
+    segment_tasks(np, lens, T, k, flags, pick_seg_len(np.N, 4LL * di.sms, seg_tile, !plain, tc.seg_div, min_tiles),
+                  !plain);
     bool all_flush = T > 0;  // every non-empty task is split and sampled
     for (int64_t t = 0; t < T; ++t)
         if (lens[t] > 0 && (np.tasks[t].flags & kTaskSampled) == 0) all_flush = false;
@@ -480,7 +487,7 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
         occ = std::max(occ, 1);
         segment_tasks(np, lens, T, k, flags,
                       pick_seg_len(np.N, static_cast<int64_t>(occ) * di.sms, seg_tile, np.fused, tc.seg_div,
-                                   tc.seg_min_tiles),
+                                   min_tiles),
                       np.fused);
     }
     const int64_t resident = static_cast<int64_t>(occ) * di.sms;
@@ -1077,8 +1084,9 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     reps = std::max(1, std::min(reps, 100));
     // Candidate shapes: the defaults, other rings and block sizes of the
     // warp-specialised form, a larger sample, the barrier form, other
-    // segment sizes for split tasks, and short segments (4 tiles), which
-    // spread a single task of a few million elements over the whole GPU.
+    // segment sizes for split tasks, and both fixed shortest segments (4
+    // tiles spread a single task of a few million elements over the whole
+    // GPU; 64 tiles keep it in fewer, unsampled segments).
     std::vector<TuneConfig> cands;
     TuneConfig d;
     cands.push_back(d);
@@ -1091,6 +1099,7 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     { TuneConfig c = d; c.defer = 0; cands.push_back(c); }
     { TuneConfig c = d; c.defer = 1; cands.push_back(c); }
     { TuneConfig c = d; c.seg_min_tiles = 4; cands.push_back(c); }
+    { TuneConfig c = d; c.seg_min_tiles = 64; cands.push_back(c); }
     PlanKey base = plan_key(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
     auto set_choice = [&](const TuneConfig& c) {
         for (auto& e : ws->tuned) {
@@ -1300,6 +1309,7 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
     view.index_bytes = idx_bytes;
     TuneConfig tc = with_env(TuneConfig{});
     tc.defer = 0;  // deferred regions are sized for a workspace, not for the static scratch
+    if (tc.seg_min_tiles == 0) tc.seg_min_tiles = 64;  // long segments: fewer candidate regions
     rc = plan_shape(h_task_lens, num_tasks, k, flags, view.plan, tc);
     if (rc) return rc;
     const Plan& pl = view.plan;
