@@ -140,9 +140,12 @@ int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const floa
  * and a message giving the bytes needed.  RADIK_PLAIN and RADIK_ASYNC are
  * rejected: the call clears the scratch state that must start at zero,
  * uploads the plan, launches, and waits for `stream` before returning.
- * The first call on each device does set-up (cudaGetSymbolAddress of the
- * static array, kernel attributes); make it before any stream capture.  A
- * capturing stream is rejected with RADIK_ERR_CAPTURE.
+ * Every call looks up the static array's address on the current device
+ * (cudaGetSymbolAddress) and sets the kernel attributes it needs; neither
+ * allocates, and a context that was reset and recreated between calls gets
+ * the new address.  The first call on a device may load the library's
+ * device code there: make it before any stream capture.  A capturing stream
+ * is rejected with RADIK_ERR_CAPTURE.
  * All calls on one device share the array: calls that overlap in time (from
  * several host threads, or on streams that are not ordered with each other)
  * race and corrupt each other's results. */
@@ -189,6 +192,11 @@ int radik_server_submit(radik_server* server, const float* d_data, int64_t rows,
  * it completed (the ticket is then released), RADIK_ERR_TIMEOUT if not yet. */
 int radik_server_wait(radik_server* server, uint64_t ticket, int64_t timeout_us);
 int radik_server_get_stats(radik_server* server, radik_server_stats* stats);
+/* Per-request latencies behind the statistics: for the requests completed
+ * since the last reset, in completion order, tickets[i] and lat_us[i]
+ * (submission to completion) for i < min(cap, *n); *n receives how many
+ * there are.  Callers group them by request shape. */
+int radik_server_get_latencies(radik_server* server, uint64_t* tickets, double* lat_us, int64_t cap, int64_t* n);
 int radik_server_reset_stats(radik_server* server);
 
 /* ---- Stage entry points: the reference kernels' own contracts ----------- */
@@ -220,6 +228,13 @@ int radik_select_bin(int32_t* d_bin_ids, int32_t* d_k_values, int32_t* d_counts,
 int radik_filter(float* d_val_out, void* d_idx_out, int idx_bytes, int32_t* d_counts, int32_t* d_boundary,
                  const float* d_data, const void* d_idx_in, const float* d_kth, const int64_t* h_task_lens,
                  int64_t num_tasks, int64_t k, int withscale, int largest, void* stream);
+
+/* Engine diagnostics (no reference counterpart): the number of CUDA
+ * allocations -- device memory and pinned host memory -- this library has
+ * made in the process so far (workspace buffers, plan staging, the
+ * host-buffer entry point's device copies, server slots).  Comparing it
+ * before and after a call shows whether that call allocated. */
+int radik_alloc_count(uint64_t* count);
 
 /* Message of the last failure on this thread ("" when none). */
 const char* radik_last_error(void);

@@ -77,6 +77,33 @@ def _check_float32(data):
                          "Convert with: data.to(torch.float32)")
 
 
+def _check_io(val_out, idx_out, val_in, idx_in, lens: np.ndarray, k: int, withidxin: bool) -> None:
+    """Buffer sizes against the batch, then placement: the kernels write
+    len(lens) * k entries of each output and read sum(lens) input elements
+    (and indices) on the current device, so a short buffer or a tensor on
+    another GPU must be refused here, not turned into a device fault.
+    Sizes are checked first (they need no GPU)."""
+    T, total = len(lens), int(lens.sum()) if len(lens) else 0
+    need = T * int(k)
+    for name, t, n in (("val_out", val_out, need), ("idx_out", idx_out, need), ("val_in", val_in, total),
+                       ("idx_in", idx_in if withidxin else None, total)):
+        if t is not None and t.numel() < n:
+            what = f"{T} tasks x k = {k}" if name in ("val_out", "idx_out") else f"sum(task_lens) = {total}"
+            raise RadiKError(f"{name} holds {t.numel()} elements; {what} needs {n}")
+    if withidxin and idx_in is None:
+        raise RadiKError("withidxin needs idx_in")
+    tensors = [("val_out", val_out), ("idx_out", idx_out), ("val_in", val_in)]
+    if withidxin:
+        tensors.append(("idx_in", idx_in))
+    for name, t in tensors:
+        _check_cuda(t, name)
+    dev = _torch().cuda.current_device()
+    for name, t in tensors:
+        if t.device.index != dev:
+            raise RadiKError(f"{name} is on cuda:{t.device.index} but the current device is cuda:{dev}; "
+                             "the kernels run on the current device")
+
+
 def _idx_bytes(dtype) -> int:
     torch = _torch()
     if dtype == torch.int32:
@@ -145,10 +172,8 @@ class RadiKWorkspace:
         keep the fastest for its shape (radik_ws_autotune); returns the chosen
         plan with its time per call ("ms")."""
         from ._lib import PlanInfo
-        _check_cuda(val_out, "val_out")
-        _check_cuda(idx_out, "idx_out")
-        _check_cuda(val_in, "val_in")
         lens = _lens_array(task_lens)
+        _check_io(val_out, idx_out, val_in, idx_in, lens, k, withidxin)
         info = PlanInfo()
         ms = ctypes.c_double()
         flags = _flags(largest, ascend, withscale, withidxin)
@@ -195,15 +220,11 @@ def topk_radix_select_(val_out, idx_out, ws: RadiKWorkspace, val_in, idx_in, tas
     ((num_tasks, k) tensors), sorted ascending when ``ascend``.  Synchronous
     like the reference unless ``sync=False``.  ``withpacking`` and
     ``vload_size_bytes`` are accepted for parity (loads are 128-bit)."""
-    _check_cuda(val_out, "val_out")
-    _check_cuda(idx_out, "idx_out")
-    _check_cuda(val_in, "val_in")
     _check_float32(val_in)
-    if withidxin:
-        _check_cuda(idx_in, "idx_in")
-        if idx_in.dtype != idx_out.dtype:
-            raise RadiKError("idx_in and idx_out must have the same element type")
     lens = _lens_array(task_lens)
+    _check_io(val_out, idx_out, val_in, idx_in, lens, k, withidxin)
+    if withidxin and idx_in.dtype != idx_out.dtype:
+        raise RadiKError("idx_in and idx_out must have the same element type")
     L = load()
     flags = _flags(largest, ascend, withscale, withidxin, plain, sync)
     check(L.radik_topk_radix_select(_ptr(val_out), _ptr(idx_out), _idx_bytes(idx_out.dtype), ws.handle,
@@ -223,15 +244,11 @@ def topk_radix_select_noalloc_(val_out, idx_out, val_in, idx_in, task_lens, k: i
     scratch must fit in 8 MiB, else RadiKError.  Calls that overlap in time
     on one device race; the first call on a device does set-up and must come
     before any stream capture."""
-    _check_cuda(val_out, "val_out")
-    _check_cuda(idx_out, "idx_out")
-    _check_cuda(val_in, "val_in")
     _check_float32(val_in)
-    if withidxin:
-        _check_cuda(idx_in, "idx_in")
-        if idx_in.dtype != idx_out.dtype:
-            raise RadiKError("idx_in and idx_out must have the same element type")
     lens = _lens_array(task_lens)
+    _check_io(val_out, idx_out, val_in, idx_in, lens, k, withidxin)
+    if withidxin and idx_in.dtype != idx_out.dtype:
+        raise RadiKError("idx_in and idx_out must have the same element type")
     L = load()
     flags = _flags(largest, ascend, withscale, withidxin)
     check(L.radik_topk_noalloc(_ptr(val_out), _ptr(idx_out), _idx_bytes(idx_out.dtype), _ptr(val_in),
@@ -445,6 +462,18 @@ class Server:
         st = ServerStats()
         check(load().radik_server_get_stats(self._h, ctypes.byref(st)))
         return {n: getattr(st, n) for n, _ in ServerStats._fields_}
+
+    def latencies(self) -> dict:
+        """Submission-to-completion latency (us) of every request completed
+        since the last reset_stats, by ticket."""
+        L = load()
+        n = ctypes.c_int64()
+        check(L.radik_server_get_latencies(self._h, None, None, 0, ctypes.byref(n)))
+        cap = int(n.value)
+        tk = (ctypes.c_uint64 * max(cap, 1))()
+        lat = (ctypes.c_double * max(cap, 1))()
+        check(L.radik_server_get_latencies(self._h, tk, lat, cap, ctypes.byref(n)))
+        return {int(tk[i]): float(lat[i]) for i in range(min(cap, int(n.value)))}
 
     def reset_stats(self) -> None:
         check(load().radik_server_reset_stats(self._h))

@@ -32,9 +32,9 @@ EXPORTS = (
     "radik_ws_plan_info", "radik_ws_autotune",
     "radik_topk_radix_select", "radik_topk", "radik_topk_host", "radik_topk_noalloc",
     "radik_count_bin_ex", "radik_count_bin", "radik_select_bin", "radik_filter",
-    "radik_last_error", "radik_status_string", "radik_version",
+    "radik_last_error", "radik_status_string", "radik_version", "radik_alloc_count",
     "radik_server_create", "radik_server_destroy", "radik_server_submit", "radik_server_wait",
-    "radik_server_get_stats", "radik_server_reset_stats",
+    "radik_server_get_stats", "radik_server_get_latencies", "radik_server_reset_stats",
 )
 
 
@@ -95,7 +95,10 @@ def _declare(L: ctypes.CDLL) -> None:
     L.radik_server_submit.argtypes = [P, P, I64, I64, I64, U32, P, P, I, ctypes.POINTER(ctypes.c_uint64)]
     L.radik_server_wait.argtypes = [P, ctypes.c_uint64, I64]
     L.radik_server_get_stats.argtypes = [P, ctypes.POINTER(ServerStats)]
+    L.radik_server_get_latencies.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
+                                             I64, ctypes.POINTER(I64)]
     L.radik_server_reset_stats.argtypes = [P]
+    L.radik_alloc_count.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
     L.radik_last_error.restype = ctypes.c_char_p
     L.radik_status_string.restype = ctypes.c_char_p
     L.radik_status_string.argtypes = [I]

@@ -33,7 +33,10 @@ def sources() -> list[pathlib.Path]:
 
 
 def deps() -> list[pathlib.Path]:
-    return sources() + sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "radik.h"]
+    """Every file the library is compiled from: the .cu sources, their
+    headers and the .inl files they include (the request server)."""
+    return (sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inl"))
+            + [ROOT / "include" / "radik.h"])
 
 
 def stale() -> bool:

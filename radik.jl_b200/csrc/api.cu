@@ -1,6 +1,7 @@
 // api.cu -- C ABI of the engine (include/radik.h): workspace, launch plans,
 // the fused single-read path, the multi-pass path and the stage entry points.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -36,6 +37,21 @@ int fail(int code, const std::string& msg) {
         if (e_ != cudaSuccess) return fail(RADIK_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
     } while (0)
 
+// Every device and pinned-host allocation the library makes goes through
+// these two, which count them (radik_alloc_count).
+std::atomic<uint64_t> g_alloc_count{0};
+
+cudaError_t counted_malloc(void** p, size_t n) {
+    g_alloc_count.fetch_add(1, std::memory_order_relaxed);
+    return cudaMalloc(p, n);
+}
+
+template <typename T>
+cudaError_t counted_malloc_host(T** p, size_t n) {
+    g_alloc_count.fetch_add(1, std::memory_order_relaxed);
+    return cudaMallocHost(reinterpret_cast<void**>(p), n);
+}
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -43,7 +59,7 @@ struct DevBuf {
         if (b <= bytes) return cudaSuccess;
         if (p) { cudaFree(p); p = nullptr; bytes = 0; }
         size_t nb = b < 256 ? 256 : b;
-        cudaError_t e = cudaMalloc(&p, nb);
+        cudaError_t e = counted_malloc(&p, nb);
         if (e == cudaSuccess) bytes = nb;
         return e;
     }
@@ -144,21 +160,19 @@ int env_int(const char* name, int dflt) {
 // Tunable shape of a plan.  Defaults are the measured best for the common
 // cases; radik_ws_autotune picks another per batch shape; environment
 // variables (RADIK_WS, RADIK_WST, RADIK_WSJ, RADIK_WSS, RADIK_WS_SAMPLE,
-// RADIK_WS_WINDOWS, RADIK_SEG_DIV, RADIK_DEFER, RADIK_SEG_MIN) override both, for
-// experiments.
+// RADIK_SEG_DIV, RADIK_DEFER, RADIK_SEG_MIN) override both, for experiments.
 struct TuneConfig {
     int form = -1;          // -1 automatic, 0 barrier form, 1 warp-specialised form
     int ws_threads = 128;   // warp-specialised: consumer threads
     int ws_j = 8;           // float4 per lane in a warp tile
     int ws_stages = 8;      // ring stages (a multiple of the consumer warps)
     int sample_max = 2048;  // single-segment sample (elements)
-    int sample_windows = 2; // digit windows of its rank threshold
     int seg_div = 3;        // work items per resident block when splitting tasks
     int defer = -1;         // deferred finish of single-segment tasks: -1 automatic, 0 no, 1 yes
     int seg_min_tiles = 0;  // shortest segment of a split task in 2048-element tiles; 0 automatic
     bool operator==(const TuneConfig& o) const {
         return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
-               sample_max == o.sample_max && sample_windows == o.sample_windows && seg_div == o.seg_div &&
+               sample_max == o.sample_max && seg_div == o.seg_div &&
                defer == o.defer && seg_min_tiles == o.seg_min_tiles;
     }
 };
@@ -169,7 +183,6 @@ TuneConfig with_env(TuneConfig c) {
     c.ws_j = env_int("RADIK_WSJ", c.ws_j);
     c.ws_stages = env_int("RADIK_WSS", c.ws_stages);
     c.sample_max = env_int("RADIK_WS_SAMPLE", c.sample_max);
-    c.sample_windows = env_int("RADIK_WS_WINDOWS", c.sample_windows);
     c.seg_div = std::max(1, env_int("RADIK_SEG_DIV", c.seg_div));
     c.defer = env_int("RADIK_DEFER", c.defer);
     c.seg_min_tiles = std::max(0, env_int("RADIK_SEG_MIN", c.seg_min_tiles));
@@ -200,7 +213,6 @@ struct Plan {
     bool ws_form = false;   // warp-specialised fused kernel
     int ws_stages = 16;     // its ring stages
     int ws_sample_max = 2048;    // its single-segment sample (elements)
-    int ws_sample_windows = 2;   // digit windows of the sample's rank threshold
     int threads = 256, vec = 16;
     int launch_threads = 256;  // threads plus the producer warp of the warp-specialised form
     uint32_t cap = 0;
@@ -419,7 +431,6 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     const int ws_threads = tc.ws_threads;
     np.ws_stages = tc.ws_stages;
     np.ws_sample_max = tc.sample_max;
-    np.ws_sample_windows = tc.sample_windows;
     const size_t seg_tile = 2048;  // segments are whole tiles of either form
     // Shortest segment.  A single task too short to give every SM a 64-tile
     // segment is cut into 4-tile segments, sampled, and merged: 2^20 to 2^24
@@ -636,7 +647,7 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
             if (ws->h_stage) cudaFreeHost(ws->h_stage);
             ws->h_stage = nullptr;
             ws->h_stage_bytes = 0;
-            e = cudaMallocHost(&ws->h_stage, desc_bytes);
+            e = counted_malloc_host(&ws->h_stage, desc_bytes);
             if (e == cudaSuccess) ws->h_stage_bytes = desc_bytes;
         }
         if (e == cudaSuccess) {
@@ -704,7 +715,6 @@ FusedParams fused_params(radik_ws* ws, float* vout, void* iout, int idx_bytes, c
     p.fail = ws->state.as<uint32_t>(L.fail);
     p.fail_any = ws->state.as<uint32_t>(StateLayout::kAny);
     p.sample_max = static_cast<uint32_t>(pl.ws_sample_max);
-    p.sample_windows = static_cast<uint32_t>(pl.ws_sample_windows);
     p.cand = ws->cand.as<uint64_t>();
     p.sort_scratch = ws->scratch.as<uint64_t>();
     p.rank_ready = ws->state.as<uint32_t>(L.rk);
@@ -895,6 +905,20 @@ int finish_sync(radik_ws* ws, cudaStream_t s) {
     return RADIK_OK;
 }
 
+// A workspace's buffers live on the device it was created on; the kernels
+// run on the current device.
+int check_ws_device(const radik_ws* ws) {
+    int dev = 0;
+    RADIK_CUDA(cudaGetDevice(&dev));
+    if (dev != ws->device) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "the workspace belongs to cuda:%d but the current device is cuda:%d",
+                      ws->device, dev);
+        return fail(RADIK_ERR_INVALID, buf);
+    }
+    return RADIK_OK;
+}
+
 int validate_lens(const int64_t* lens, int64_t T, int64_t* maxlen) {
     *maxlen = 0;
     for (int64_t t = 0; t < T; ++t) {
@@ -915,6 +939,12 @@ extern "C" {
 const char* radik_version(void) { return "radik-b200 0.1.0 (sm_100a)"; }
 
 const char* radik_last_error(void) { return g_last_error.c_str(); }
+
+int radik_alloc_count(uint64_t* count) {
+    if (!count) return fail(RADIK_ERR_INVALID, "NULL argument");
+    *count = g_alloc_count.load(std::memory_order_relaxed);
+    return RADIK_OK;
+}
 
 const char* radik_status_string(int st) {
     switch (st) {
@@ -941,7 +971,7 @@ int radik_ws_create(int64_t n, int64_t num_tasks, int index_bytes, radik_ws** ou
     ws->n = n;
     ws->num_tasks = num_tasks;
     ws->index_bytes = index_bytes;
-    if (cudaMallocHost(&ws->h_err, sizeof(uint32_t)) != cudaSuccess) {
+    if (counted_malloc_host(&ws->h_err, sizeof(uint32_t)) != cudaSuccess) {
         delete ws;
         return fail(RADIK_ERR_OOM, "pinned allocation failed");
     }
@@ -1015,8 +1045,10 @@ int radik_ws_prepare(radik_ws* ws, const int64_t* h_task_lens, int64_t num_tasks
     if (!ws || (!h_task_lens && num_tasks > 0)) return fail(RADIK_ERR_INVALID, "NULL argument");
     if (k < 0) return fail(RADIK_ERR_INVALID, "k must be non-negative");
     if (idx_bytes != 4 && idx_bytes != 8) return fail(RADIK_ERR_INVALID, "index width must be 4 or 8 bytes");
+    int rc = check_ws_device(ws);
+    if (rc) return rc;
     int64_t maxlen = 0;
-    int rc = validate_lens(h_task_lens, num_tasks, &maxlen);
+    rc = validate_lens(h_task_lens, num_tasks, &maxlen);
     if (rc) return rc;
     if (maxlen > ws->n || num_tasks > ws->num_tasks)
         return fail(RADIK_ERR_WS_TOO_SMALL, "workspace requires n >= max(task_lens) and num_tasks <= its num_tasks");
@@ -1033,12 +1065,14 @@ int radik_topk_radix_select(float* d_val_out, void* d_idx_out, int idx_bytes, ra
     if ((flags & RADIK_WITHIDXIN) && !d_idx_in) return fail(RADIK_ERR_INVALID, "WITHIDXIN needs idx_in");
     if (num_tasks == 0 || k == 0) return RADIK_OK;
     if (!d_val_out || !d_idx_out || !h_task_lens) return fail(RADIK_ERR_INVALID, "NULL output or task_lens");
+    int rc = check_ws_device(ws);
+    if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     ws->last_stream = s;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cap);
     int64_t maxlen = 0;
-    int rc = validate_lens(h_task_lens, num_tasks, &maxlen);
+    rc = validate_lens(h_task_lens, num_tasks, &maxlen);
     if (rc) return rc;
     if (maxlen > ws->n || num_tasks > ws->num_tasks)
         return fail(RADIK_ERR_WS_TOO_SMALL, "workspace requires n >= max(task_lens) and num_tasks <= its num_tasks");
@@ -1187,6 +1221,8 @@ int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const floa
                       static_cast<long long>(indices_len), static_cast<long long>(data_len));
         return fail(RADIK_ERR_INVALID, buf);
     }
+    int rc = check_ws_device(ws);
+    if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const bool with_idx = h_indices && indices_len > 0;
     const size_t out_n = static_cast<size_t>(num_tasks) * static_cast<size_t>(k);
@@ -1201,7 +1237,7 @@ int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const floa
                                    cudaMemcpyHostToDevice, s));
     uint32_t flags = (largest ? RADIK_LARGEST : 0u) | (rev ? 0u : RADIK_ASCEND) | RADIK_ASYNC;
     if (with_idx) flags |= RADIK_WITHIDXIN;
-    int rc = radik_topk_radix_select(ws->io_vout.as<float>(), ws->io_iout.p, idx_bytes, ws, ws->io_in.as<float>(),
+    rc = radik_topk_radix_select(ws->io_vout.as<float>(), ws->io_iout.p, idx_bytes, ws, ws->io_in.as<float>(),
                                      with_idx ? ws->io_idx.p : nullptr, h_task_lens, num_tasks, k, flags, stream);
     if (rc) return rc;
     if (out_n) {
@@ -1227,36 +1263,29 @@ int radik_topk_host(float* h_val_out, void* h_idx_out, int idx_bytes, const floa
 
 namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB per device
-constexpr int kNoAllocMaxDevices = 64;
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 namespace {
 
-std::mutex g_noalloc_mu;
-char* g_noalloc_base[kNoAllocMaxDevices] = {};
-
-// Per-device set-up: the device address of the static scratch and the
-// shared-memory attribute of the sampling kernels.  Runs once per device, on
-// the first call there.
-int noalloc_setup(int dev, char** base) {
-    if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(RADIK_ERR_INVALID, "device ordinal out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_base[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(RADIK_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
-        const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
-        for (bool scale : {false, true}) {
-            e = cudaFuncSetAttribute(reinterpret_cast<const void*>(pick_sample(scale)),
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ssmem));
-            if (e != cudaSuccess) return fail(RADIK_ERR_CUDA, std::string("sampling kernel: ") + cudaGetErrorString(e));
-        }
-        g_noalloc_base[dev] = static_cast<char*>(p);
+// Set-up of an allocation-free call on the current device: the device
+// address of the static scratch (in host code the array's name is only a
+// host-side stand-in, never a device address) and the sampling kernels'
+// shared-memory attribute.  Redone on every call -- neither allocates -- so
+// that a context reset between calls cannot leave a stale address behind.
+int noalloc_setup(char** base) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(RADIK_ERR_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+    const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
+    for (bool scale : {false, true}) {
+        e = cudaFuncSetAttribute(reinterpret_cast<const void*>(pick_sample(scale)),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(ssmem));
+        if (e != cudaSuccess) return fail(RADIK_ERR_CUDA, std::string("sampling kernel: ") + cudaGetErrorString(e));
     }
-    *base = g_noalloc_base[dev];
+    *base = static_cast<char*>(p);
     return RADIK_OK;
 }
 
@@ -1297,7 +1326,7 @@ int radik_topk_noalloc(float* d_val_out, void* d_idx_out, int idx_bytes, const f
     int dev = 0;
     RADIK_CUDA(cudaGetDevice(&dev));
     char* base = nullptr;
-    rc = noalloc_setup(dev, &base);
+    rc = noalloc_setup(&base);
     if (rc) return rc;
 
     // A workspace view whose buffers all point into the static scratch; it

@@ -300,6 +300,66 @@ __device__ uint64_t block_rank_threshold(const uint64_t* buf, uint32_t n, uint32
     return keep_from;
 }
 
+// Largest T such that at least r of the warp's values x[] (NV per lane,
+// padding 0, 1 <= r <= number of real values) are >= T: the r-th largest
+// value, built two bits at a time below the values' common prefix (three
+// counts per step, one warp reduction each).  With kExact, the search also
+// stops at the first T with exactly r values >= T (any such T separates the
+// r largest from the rest).  Only the calling warp takes part.
+template <int NV, bool kExact = false>
+__device__ __forceinline__ uint32_t warp_rank_search(const uint32_t (&x)[NV], uint32_t r) {
+    uint32_t vor = 0u, vand = ~0u;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        vor |= x[j];
+        if (x[j] != 0u) vand &= x[j];
+    }
+    vor = __reduce_or_sync(kFullMask, vor);
+    vand = __reduce_and_sync(kFullMask, vand);
+    const uint32_t diff = vor ^ vand;
+    if (diff == 0u) return vand;
+    int b = 31 - __clz(diff);                 // highest bit where the values differ
+    uint32_t T = vand & ~((2u << b) - 1u);    // their common prefix: every value is >= T
+    for (; b >= 1; b -= 2) {
+        const uint32_t c1 = T | (1u << (b - 1)), c2 = T | (2u << (b - 1)), c3 = T | (3u << (b - 1));
+        uint32_t n1 = 0, n2 = 0, n3 = 0;
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+            n1 += x[j] >= c1 ? 1u : 0u;
+            n2 += x[j] >= c2 ? 1u : 0u;
+            n3 += x[j] >= c3 ? 1u : 0u;
+        }
+        n1 = __reduce_add_sync(kFullMask, n1);
+        n2 = __reduce_add_sync(kFullMask, n2);
+        n3 = __reduce_add_sync(kFullMask, n3);
+        const uint32_t nT = n3 >= r ? n3 : (n2 >= r ? n2 : (n1 >= r ? n1 : 0u));
+        T = n3 >= r ? c3 : (n2 >= r ? c2 : (n1 >= r ? c1 : T));
+        if (kExact && nT == r) return T;
+    }
+    if (b == 0) {
+        const uint32_t c1 = T | 1u;
+        uint32_t n1 = 0;
+#pragma unroll
+        for (int j = 0; j < NV; ++j) n1 += x[j] >= c1 ? 1u : 0u;
+        if (__reduce_add_sync(kFullMask, n1) >= r) T = c1;
+    }
+    return T;
+}
+
+// The r-th largest (1-based, 1 <= r <= n) of the high words of gm[0, n)
+// (n <= 32 * NV), found by the calling warp (warp_rank_search).
+template <int NV>
+__device__ __forceinline__ uint32_t warp_rank_value(const uint64_t* gm, uint32_t n, uint32_t r) {
+    const uint32_t lane = lane_id();
+    uint32_t x[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+        const uint32_t i = static_cast<uint32_t>(j) * 32u + lane;
+        x[j] = i < n ? static_cast<uint32_t>(gm[i] >> 32) : 0u;  // padding 0 is below every candidate T
+    }
+    return warp_rank_search<NV>(x, r);
+}
+
 constexpr uint32_t kWarpBisect = 512;  // boundary-bin entries one warp finishes (16 per lane)
 
 // Bound of the k best among buf[0, n) (unique composites in shared memory,

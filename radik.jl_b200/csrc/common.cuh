@@ -34,6 +34,11 @@ __device__ __forceinline__ uint32_t key_of_bits(uint32_t b) {
     return b ^ (static_cast<uint32_t>(static_cast<int32_t>(b) >> 31) | 0x80000000u);
 }
 
+// The Float32 whose key is `key` (inverse of key_of_bits).
+__device__ __forceinline__ float value_of_key(uint32_t key) {
+    return __uint_as_float((key & 0x80000000u) ? (key ^ 0x80000000u) : ~key);
+}
+
 __device__ __forceinline__ bool is_nan_bits(uint32_t b) { return (b & 0x7fffffffu) > 0x7f800000u; }
 
 // Score parameters of one call (same for all tasks).

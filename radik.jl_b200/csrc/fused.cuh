@@ -89,7 +89,6 @@ struct FusedParams {
     uint32_t* fail;          // [T] seeded threshold too high
     uint32_t* fail_any;      // [1] some task is flagged in `fail` (the retry launch exits at once otherwise)
     uint32_t sample_max;     // warp-specialised kernel: most elements of a single-segment task's sample
-    uint32_t sample_windows; // digit windows of its rank threshold
     uint32_t* work_counter;  // [1]
     uint64_t* cand;          // candidate regions
     uint64_t* sort_scratch;  // [gridDim.x * kmax] (kmax > 4096 only)
@@ -272,6 +271,194 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
     write_row<THREADS, kFromScore>(p, tv, sorted, m);
 }
 
+// Bucket finish (finish_by_buckets): largest k, and largest bin whose
+// entries it orders by scanning the bin.
+constexpr uint32_t kBucketMaxK = 512;
+constexpr uint32_t kBucketScanMax = 64;
+
+// Output row of a single-segment task from its candidates buf[0, cnt) (unique
+// composites), with one histogram pass and no sorting network:
+//   1. the candidates are counted in 256 bins of the (up to) 8 score bits
+//      below their common prefix (bins follow the composite order and keep
+//      equal scores together);
+//   2. warp 0 scans the bins from the top: the bin b* holding rank
+//      m = min(cnt, want), the entries above each bin (its bucket offset in
+//      composite order) and how many of b*'s entries are in (need);
+//   3. the entries of bins >= b* are scattered to their buckets;
+//   4. an entry's rank inside its bin (by composite, then by output order)
+//      comes from a scan of its bin's few entries; b*'s entries are in when
+//      their rank is below need.  The row position follows: bins are in score
+//      order, so a descending row (largest, !ascend / smallest, ascend) is the
+//      composite order itself, and an ascending-score row is the bins in
+//      reverse with each bin's entries by ascending (score, position).
+// Returns false, having written nothing, when a bin at or above b* holds more
+// than kBucketScanMax entries (many ties or clustered values) or the scratch
+// behind the candidates is too small; the caller then finishes by radix
+// selection.  Unscaled scores only (a value is its key's preimage; the element
+// itself where the key is the NaN substitute's).  Slots m..k-1 are padded
+// with 0 / -1 (src/algorithm.jl:358-365).  All threads must call.
+template <int THREADS>
+__device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint64_t* buf, uint32_t cnt, uint32_t want,
+                                  FusedShared<THREADS>& sh) {
+    constexpr uint32_t Q = (kBucketMaxK + kBucketScanMax + THREADS - 1) / THREADS;  // bucket entries per thread
+    const uint32_t tid = threadIdx.x;
+    const uint32_t m = cnt < want ? cnt : want;
+    // Scratch behind the candidates: the buckets, then bucket offsets and
+    // scatter cursors (256 words each).
+    const uint32_t boff = (cnt + 1u) & ~1u;
+    const uint32_t words_off = boff + m + kBucketScanMax;
+    if (static_cast<size_t>(words_off) + 256u > p.cap) return false;  // uniform: no barrier taken yet
+    uint64_t* bucket = buf + boff;
+    uint32_t* off = reinterpret_cast<uint32_t*>(buf + words_off);
+    uint32_t* cur = off + 256;
+    uint32_t* hist = sh.bs.hist;
+
+    uint64_t vor = 0, vand = ~0ull;
+    for (uint32_t i = tid; i < cnt; i += THREADS) {
+        const uint64_t c = buf[i];
+        vor |= c;
+        vand &= c;
+    }
+    block_or_and<THREADS>(vor, vand, sh.bs);
+    const uint64_t diff = vor ^ vand;
+    const int top = diff ? 63 - __clzll(static_cast<long long>(diff)) : 0;
+    // Bins cut the scores only (a run of equal scores stays in one bin) unless
+    // every candidate has the same score; then they cut the positions, and
+    // either row order is the composite order (ascending positions).
+    const bool one_score = top < 32;
+    const int w = one_score ? (top + 1 < 8 ? top + 1 : 8) : (top - 31 < 8 ? top - 31 : 8);
+    const int shift = top + 1 - w;
+    const uint32_t nb = 1u << w, bmask = nb - 1u;
+    for (uint32_t b = tid; b < nb; b += THREADS) {
+        hist[b] = 0;
+        cur[b] = 0;
+    }
+    block_sync<THREADS>();
+    for (uint32_t i = tid; i < cnt; i += THREADS) atomicAdd(hist + (static_cast<uint32_t>(buf[i] >> shift) & bmask), 1u);
+    block_sync<THREADS>();
+    if (tid < 32) {
+        // Bins from the top: lane l takes bins nb-1-l*per ... (per <= 8).
+        const uint32_t lane = tid, per = (nb + 31u) / 32u;
+        uint32_t sum = 0;
+        for (uint32_t j = 0; j < per; ++j) {
+            const uint32_t rb = lane * per + j;
+            sum += rb < nb ? hist[nb - 1u - rb] : 0u;
+        }
+        const uint32_t incl = warp_inclusive_scan<true>(sum);
+        uint32_t run = incl - sum;  // entries in the bins above this lane's
+        uint32_t bstar = 0xffffffffu, need = 0, big = 0;
+        for (uint32_t j = 0; j < per; ++j) {
+            const uint32_t rb = lane * per + j;
+            if (rb >= nb) break;
+            const uint32_t b = nb - 1u - rb, h = hist[b];
+            off[b] = run;
+            if (run < m) {  // a bin that holds some of the m best
+                big = h > big ? h : big;
+                if (run + h >= m) {
+                    bstar = b;
+                    need = m - run;
+                }
+            }
+            run += h;
+        }
+        big = __reduce_max_sync(kFullMask, big);
+        const uint32_t who = __ballot_sync(kFullMask, bstar != 0xffffffffu);
+        if (who != 0u) {
+            const uint32_t src = __ffs(who) - 1u;
+            bstar = __shfl_sync(kFullMask, bstar, src);
+            need = __shfl_sync(kFullMask, need, src);
+        }
+        if (lane == 0) {
+            sh.bs.bc32[0] = bstar;  // 0xffffffff: m == 0
+            sh.bs.bc32[1] = need;
+            sh.bs.bc32[2] = big > kBucketScanMax ? 1u : 0u;
+        }
+    }
+    block_sync<THREADS>();
+    const uint32_t bstar = sh.bs.bc32[0], need = sh.bs.bc32[1];
+    if (sh.bs.bc32[2] != 0u) return false;  // uniform; buf[0, cnt) is untouched
+    const uint32_t nsel = bstar == 0xffffffffu ? 0u : off[bstar] + hist[bstar];  // entries of bins >= b*
+    if (nsel != 0u) {
+        for (uint32_t i = tid; i < cnt; i += THREADS) {
+            const uint64_t c = buf[i];
+            const uint32_t b = static_cast<uint32_t>(c >> shift) & bmask;
+            if (b >= bstar) bucket[off[b] + atomicAdd(cur + b, 1u)] = c;
+        }
+    }
+    block_sync<THREADS>();
+    // Ranks inside the bins by composite (descending); the need-th of b*
+    // is the bound tau of the m best.
+    uint64_t ce[Q];
+    uint32_t rd[Q];
+#pragma unroll
+    for (int q = 0; q < static_cast<int>(Q); ++q) {
+        const uint32_t s = static_cast<uint32_t>(q) * THREADS + tid;
+        ce[q] = s < nsel ? bucket[s] : 0ull;
+        rd[q] = 0;
+        if (s < nsel) {
+            const uint32_t b = static_cast<uint32_t>(ce[q] >> shift) & bmask;
+            const uint32_t lo = off[b], hi = lo + hist[b];
+            for (uint32_t j = lo; j < hi; ++j) rd[q] += bucket[j] > ce[q] ? 1u : 0u;
+            if (b == bstar && rd[q] == need - 1u) sh.gthr = ce[q];
+        }
+    }
+    block_sync<THREADS>();
+    const uint64_t tau = sh.gthr;
+    const bool same_order = one_score || (tv.sp.flip == 0u) != tv.ascend;
+    const uint32_t nan_key = key_of_bits(tv.sp.nan_bits);
+#pragma unroll
+    for (int q = 0; q < static_cast<int>(Q); ++q) {
+        const uint32_t s = static_cast<uint32_t>(q) * THREADS + tid;
+        if (s >= nsel) continue;
+        const uint64_t c = ce[q];
+        const uint32_t b = static_cast<uint32_t>(c >> shift) & bmask;
+        if (b == bstar && c < tau) continue;  // below the m best
+        const uint32_t sel_b = b == bstar ? need : hist[b];
+        uint32_t o;
+        if (same_order) {
+            o = off[b] + rd[q];
+        } else {
+            // Ascending scores: the bins below this one come first, then this
+            // bin's selected entries by ascending (score, position).
+            const uint32_t lo = off[b], hi = lo + hist[b];
+            const uint32_t sc = static_cast<uint32_t>(c >> 32), pc = composite_pos(c);
+            uint32_t ra = 0;
+            for (uint32_t j = lo; j < hi; ++j) {
+                const uint64_t y = bucket[j];
+                const uint32_t sy = static_cast<uint32_t>(y >> 32);
+                const bool in = b != bstar || y >= tau;
+                ra += (in && (sy < sc || (sy == sc && composite_pos(y) < pc))) ? 1u : 0u;
+            }
+            o = m - off[b] - sel_b + ra;
+        }
+        uint32_t pos = composite_pos(c);
+        if (pos >= static_cast<uint64_t>(tv.len) || o >= m) {  // never expected; keep accesses in bounds
+            record_error(p.err, pos >= static_cast<uint64_t>(tv.len) ? kErrBounds : kErrInternal);
+            continue;
+        }
+        const uint32_t key = static_cast<uint32_t>(c >> 32) ^ tv.sp.flip;
+        const float val = (key == nan_key) ? tv.data[pos] : value_of_key(key);
+        int64_t idx;
+        if (tv.iin) {
+            idx = (p.idx_bytes == 8) ? static_cast<const int64_t*>(tv.iin)[pos]
+                                     : static_cast<int64_t>(static_cast<const int32_t*>(tv.iin)[pos]);
+        } else {
+            idx = static_cast<int64_t>(pos) + 1;  // 1-based position (filter.jl:76-77)
+        }
+        tv.vout[o] = val;
+        if (p.idx_bytes == 8) static_cast<int64_t*>(tv.iout)[o] = idx;
+        else static_cast<int32_t*>(tv.iout)[o] = static_cast<int32_t>(idx);
+    }
+    if (cnt < want && tid == 0) record_error(p.err, kErrInternal);  // the caller redoes a short count
+    for (uint32_t j = m + tid; j < tv.k; j += THREADS) {
+        tv.vout[j] = 0.0f;
+        if (p.idx_bytes == 8) static_cast<int64_t*>(tv.iout)[j] = -1;
+        else static_cast<int32_t*>(tv.iout)[j] = -1;
+    }
+    block_sync<THREADS>();  // buf and the block scratch are reused by the caller
+    return true;
+}
+
 // Shared count, clamped to the buffer (appends past cap were dropped and
 // recorded); all threads must call.
 template <int THREADS>
@@ -315,6 +502,24 @@ __device__ uint32_t shrink_final(const FusedParams& p, uint32_t k, uint64_t* buf
     if (threadIdx.x == 0) sh.cnt = m;
     block_sync<THREADS>();
     return m;
+}
+
+// Finishes a single-segment task whose candidates are buf[0, sh.cnt) (a
+// superset of its best min(len, k)): for k <= 512 by one histogram pass and
+// buckets (finish_by_buckets) when no bin is crowded, else by exact radix
+// selection (shrink_final) then finish_task.  All threads must call.
+template <int THREADS, bool kScale>
+__device__ void finish_candidates(const FusedParams& p, const TaskView& tv, uint64_t* buf, FusedShared<THREADS>& sh) {
+    const uint32_t k = tv.k;
+    const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
+    const uint32_t cnt = buffer_count<THREADS>(p, sh);
+    if constexpr (!kScale) {
+        if (want <= kBucketMaxK && finish_by_buckets<THREADS>(p, tv, buf, cnt, want, sh)) return;
+    }
+    uint64_t kth = 0;
+    const uint32_t m = shrink_final<THREADS>(p, k, buf, sh, &kth);
+    if (m != want && threadIdx.x == 0) record_error(p.err, kErrInternal);
+    finish_task<THREADS, !kScale>(p, tv, buf, m < want ? m : want, sh);
 }
 
 // Starting threshold of a single-segment task from a sample of `S` of its
@@ -401,10 +606,6 @@ struct FastFilter {
     bool nan_pass;
     float4 pad4;      // value that never passes (fills past the end of a segment)
 };
-
-__device__ __forceinline__ float value_of_key(uint32_t key) {
-    return __uint_as_float((key & 0x80000000u) ? (key ^ 0x80000000u) : ~key);
-}
 
 template <bool kScale>
 __device__ __forceinline__ FastFilter make_fast_filter(uint64_t thr, const ScoreParams& sp, float scaler) {
@@ -759,11 +960,7 @@ __global__ void __launch_bounds__(THREADS, (THREADS >= 512 ? 1 : 3)) fused_topk_
         }
 
         if (!multi) {
-            uint64_t kth = 0;
-            const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
-            const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh, &kth);
-            if (m != want && tid == 0) record_error(p.err, kErrInternal);
-            finish_task<THREADS, !kScale>(p, tv, s_buf, m < want ? m : want, sh);
+            finish_candidates<THREADS, kScale>(p, tv, s_buf, sh);
         } else {
             // Multi-segment task: publish this segment's k-th composite, append
             // the survivors to the task's candidate region, count the segment.

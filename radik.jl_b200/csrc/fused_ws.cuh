@@ -107,14 +107,18 @@ __device__ __forceinline__ bool ws_warp_wait(uint64_t* bar, uint32_t parity, uin
 // Sample of a single-segment task: chunks of kSampleChunkLen consecutive
 // elements spread evenly over the task (p.sample_max <= kSampleMax elements
 // for tasks of at least 16 times that, half as many down to 8 times the
-// half, none below; the first tiles of the task in the ring).  The consumers take the maximum
-// score of every 4 consecutive sampled elements (a group) and start from the
-// lower edge of the digit bin holding the r-th largest group maximum: at
-// least r groups, hence at least r sampled elements, score at or above it.
+// half, none below; the first tiles of the task in the ring).  The consumers
+// take the maximum score of every 4 consecutive sampled elements (a group)
+// and keep every element scoring at least the r-th largest group maximum
+// (found exactly by one warp, warp_rank_value): at least r groups, hence at
+// least r sampled elements, score at or above it.
 // With lam = k * samples / len sampled elements expected at or above the
-// task's k-th score, r = lam + 2 sqrt(lam) + 3 leaves a small chance (about
-// 0.5% at lam = 8) that the threshold is too high; the task is then
-// recomputed without it, so results never depend on the sample.
+// task's k-th score, the threshold is too high only when at least r of them
+// fall in the sample: r = lam + 5 sqrt(lam) + 3 makes that a Poisson tail of
+// about 4e-7 at lam = 8.  A task that fails is redone from global memory
+// (attempt 1 from rank 2r + 8 of the same sample, then with no threshold),
+// so results never depend on the sample; but one such redo delays its whole
+// batch, so the tail must stay far below one per batch of a thousand tasks.
 constexpr uint32_t kSampleChunkLen = 64;
 constexpr uint32_t kSampleMax = 4096;
 
@@ -131,7 +135,7 @@ __device__ __forceinline__ uint32_t ws_sample_len(const FusedParams& p, const Fu
 __device__ __forceinline__ uint32_t ws_sample_rank(const FusedTask& td, uint32_t slen) {
     if (slen == 0) return 0u;
     const float lam = static_cast<float>(td.k) * static_cast<float>(slen) / static_cast<float>(td.len);
-    const uint32_t r = static_cast<uint32_t>(ceilf(lam + 2.0f * sqrtf(lam) + 3.0f));
+    const uint32_t r = static_cast<uint32_t>(ceilf(lam + 5.0f * sqrtf(lam) + 3.0f));
     return r <= slen / 4 / 4 ? r : 0u;  // at most a quarter of the groups
 }
 
@@ -405,11 +409,11 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                     block_sync<THREADS>();
                     thr = sh.thr;
                 } else if (ns != 0 && attempt < 2) {
-                    // Group maxima of 4 consecutive samples, then the lower edge
-                    // of the bin holding the rr-th largest.
-                    const uint32_t rr = attempt == 0 ? sample_r : 4 * sample_r + 16;
+                    // Group maxima of 4 consecutive samples, then the exact
+                    // rr-th largest of them (warp 0): every element scoring at
+                    // least that passes.
+                    const uint32_t rr = attempt == 0 ? sample_r : 2 * sample_r + 8;
                     const uint32_t ngroups = slen / 4;
-                    uint64_t vor = 0, vand = ~0ull;
                     const uint32_t s = (static_cast<uint32_t>(warp) + NCW - gbase % NCW) % NCW;  // my sample tile
                     if (attempt == 1) {
                         const int64_t mis = static_cast<int64_t>((reinterpret_cast<uintptr_t>(tv.data) >> 2) & 3);
@@ -422,10 +426,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                             const uint32_t b = score_of<kScale>(__float_as_uint(f.y), scaler, tv.sp);
                             const uint32_t cc = score_of<kScale>(__float_as_uint(f.z), scaler, tv.sp);
                             const uint32_t ee = score_of<kScale>(__float_as_uint(f.w), scaler, tv.sp);
-                            const uint64_t gm = static_cast<uint64_t>(max(max(a, b), max(cc, ee))) << 32;
-                            s_buf[gi] = gm;
-                            vor |= gm;
-                            vand &= gm;
+                            s_buf[gi] = static_cast<uint64_t>(max(max(a, b), max(cc, ee))) << 32;
                         }
                     } else if (s < ns) {
                         const uint32_t gt = gbase + s;
@@ -439,22 +440,18 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                             const uint32_t b = score_of<kScale>(__float_as_uint(f.y), scaler, tv.sp);
                             const uint32_t c = score_of<kScale>(__float_as_uint(f.z), scaler, tv.sp);
                             const uint32_t e = score_of<kScale>(__float_as_uint(f.w), scaler, tv.sp);
-                            const uint64_t gm = static_cast<uint64_t>(max(max(a, b), max(c, e))) << 32;
-                            s_buf[s * TW4 + j * 32 + lane] = gm;
-                            vor |= gm;
-                            vand &= gm;
+                            s_buf[s * TW4 + j * 32 + lane] = static_cast<uint64_t>(max(max(a, b), max(c, e))) << 32;
                         }
                         __syncwarp();
                         if (lane == 0) mbar_arrive(empty + st);
                     }
-                    block_or_and<THREADS>(vor, vand, sh.f.bs);  // barriers: the maxima are in s_buf
-                    if (rr <= ngroups / 2) {
-                        const uint64_t kf =
-                            block_rank_threshold<THREADS>(s_buf, ngroups, rr, p.sample_windows > 2 ? rr + rr / 2 + 2 : 4 * rr,
-                                                          vand, vor, sh.f.bs, static_cast<int>(p.sample_windows));
-                        thr = kf > 0 ? kf - 1 : 0ull;
-                        thr_used = thr != 0;
+                    block_sync<THREADS>();  // the maxima are in s_buf
+                    if (warp == 0 && rr <= ngroups / 2) {
+                        const uint32_t sv = ngroups <= 512 ? warp_rank_value<16>(s_buf, ngroups, rr)
+                                                           : warp_rank_value<32>(s_buf, ngroups, rr);
+                        thr = sv != 0u ? (static_cast<uint64_t>(sv) << 32) - 1u : 0ull;
                     }
+                    thr_used = true;  // when warp 0 found one (published below)
                 }
                 block_sync<THREADS>();
                 if (tid == 0) {
@@ -464,6 +461,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                     sh.arrived = 0;
                 }
                 block_sync<THREADS>();
+                thr = sh.thr;  // warp 0's sampled threshold reaches every warp
+                thr_used = thr_used && thr != 0;
                 wcnt = 0;
 
                 // Head [s0, a0) and tail [a1, s1): fewer than 4 elements each (warp 0).
@@ -637,11 +636,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
                     else record_error(p.err, kErrInternal);
                 }
             } else if (!multi) {
-                uint64_t kth = 0;
-                const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
-                const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
-                if (m != want && tid == 0) record_error(p.err, kErrInternal);
-                finish_task<THREADS, !kScale>(p, tv, s_buf, m < want ? m : want, sh.f);
+                finish_candidates<THREADS, kScale>(p, tv, s_buf, sh.f);
             } else {
                 // Multi-segment task: publish this segment's k-th composite, append
                 // the survivors to the task's candidate region, count the segment.
@@ -758,7 +753,6 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
             const int t = static_cast<int>(v - 1u);
             const FusedTask td = p.tasks[t];
             const TaskView tv = task_view<kScale>(p, t, td);
-            const uint32_t k = tv.k;
             uint32_t n = __ldcg(p.task_cnt + t);
             if (n > p.cap) {  // never expected: the streaming block kept at most cap
                 if (tid == 0) record_error(p.err, kErrCapacity);
@@ -769,11 +763,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
             for (uint32_t i = tid; i < n; i += THREADS) s_buf[i] = __ldcg(src + i);
             if (tid == 0) sh.f.cnt = n;
             block_sync<THREADS>();
-            uint64_t kth = 0;
-            const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
-            const uint32_t m = shrink_final<THREADS>(p, k, s_buf, sh.f, &kth);
-            if (m != want && tid == 0) record_error(p.err, kErrInternal);
-            finish_task<THREADS, !kScale>(p, tv, s_buf, m < want ? m : want, sh.f);
+            finish_candidates<THREADS, kScale>(p, tv, s_buf, sh.f);
         }
     }
 }

@@ -67,7 +67,9 @@ struct radik_server {
     uint64_t submitted = 0, completed = 0, batches = 0, rows = 0;
     double elements = 0;
     std::vector<double> lat_us;
+    std::vector<uint64_t> lat_ticket;  // ticket of lat_us[i]
     std::string worker_error;
+    size_t pool_bytes = 0;  // device bytes of the slots' workspaces, updated by the worker under mu
 };
 
 namespace {
@@ -82,13 +84,15 @@ size_t server_pool_bytes(radik_server* sv) {
     return b;
 }
 
-// Enqueues one batch (the requests in `ids`, all of one group) on a free slot.
-int server_launch(radik_server* sv, ServerSlot& sl, const std::vector<uint64_t>& ids) {
-    const ServerReq& r0 = sv->reqs[ids[0]];
+// Enqueues one batch (copies of its requests, all of one group) on a slot
+// reserved for it.  Runs without the server's lock: it touches only the
+// slot, which no other thread uses while it is reserved.
+int server_launch(ServerSlot& sl, const std::vector<ServerReq>& batch) {
+    const ServerReq& r0 = batch[0];
     int64_t T = 0, maxlen = 0;
-    for (uint64_t id : ids) {
-        T += sv->reqs[id].rows;
-        maxlen = std::max(maxlen, sv->reqs[id].row_len);
+    for (const ServerReq& r : batch) {
+        T += r.rows;
+        maxlen = std::max(maxlen, r.row_len);
     }
     std::vector<int64_t> lens;
     lens.reserve(T);
@@ -96,12 +100,11 @@ int server_launch(radik_server* sv, ServerSlot& sl, const std::vector<uint64_t>&
         if (sl.h_io) cudaFreeHost(sl.h_io);
         sl.h_io = nullptr;
         sl.h_io_cap = 0;
-        RADIK_CUDA(cudaMallocHost(&sl.h_io, sizeof(FusedTaskIO) * T));
+        RADIK_CUDA(counted_malloc_host(&sl.h_io, sizeof(FusedTaskIO) * T));
         sl.h_io_cap = static_cast<size_t>(T);
     }
     int64_t row = 0;
-    for (uint64_t id : ids) {
-        const ServerReq& r = sv->reqs[id];
+    for (const ServerReq& r : batch) {
         for (int64_t i = 0; i < r.rows; ++i, ++row) {
             lens.push_back(r.row_len);
             FusedTaskIO& io = sl.h_io[row];
@@ -152,6 +155,7 @@ void server_worker(radik_server* sv) {
                 sv->rows += static_cast<uint64_t>(r.rows);
                 sv->elements += static_cast<double>(r.rows) * static_cast<double>(r.row_len);
                 sv->lat_us.push_back(std::chrono::duration<double, std::micro>(r.t_done - r.t_submit).count());
+                sv->lat_ticket.push_back(id);
             }
             sv->in_flight -= sl.mem;
             sl.mem = 0;
@@ -186,7 +190,27 @@ void server_worker(radik_server* sv) {
                 it = sv->pending.erase(it);
             }
             if (ids.empty()) break;  // admission: wait for memory to free up
-            const int rc = server_launch(sv, sl, ids);
+            // Reserve the slot and its memory, then launch without the lock so
+            // that submitters and waiters are not held up by the plan build,
+            // the uploads or a workspace that grows.
+            std::vector<ServerReq> batch;
+            batch.reserve(ids.size());
+            for (uint64_t id : ids) batch.push_back(sv->reqs[id]);
+            sl.busy = true;
+            sl.mem = mem;
+            sv->in_flight += mem;
+            lk.unlock();
+            const int rc = server_launch(sl, batch);
+            std::string err;
+            if (rc != RADIK_OK) {
+                err = g_last_error;
+                // Kernels of the batch may already be enqueued: the callers'
+                // buffers stay in use until they are done.
+                cudaStreamSynchronize(sl.stream);
+                cudaGetLastError();
+            }
+            lk.lock();
+            sv->pool_bytes = server_pool_bytes(sv);
             if (rc != RADIK_OK) {
                 const auto now = ServerClock::now();
                 for (uint64_t id : ids) {
@@ -195,14 +219,14 @@ void server_worker(radik_server* sv) {
                     r.status = rc;
                     r.t_done = now;
                 }
-                sv->worker_error = g_last_error;
+                sv->worker_error = err;
+                sl.busy = false;
+                sv->in_flight -= sl.mem;
+                sl.mem = 0;
                 sv->cv_done.notify_all();
                 continue;
             }
             sl.reqs = std::move(ids);
-            sl.mem = mem;
-            sl.busy = true;
-            sv->in_flight += mem;
             sv->batches += 1;
             progress = true;
         }
@@ -241,7 +265,7 @@ int radik_server_create(const radik_server_config* cfg, radik_server** out) {
         int rc = RADIK_OK;
         if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl.done_ev, cudaEventDisableTiming) != cudaSuccess ||
-            cudaMallocHost(&sl.h_err, sizeof(uint32_t)) != cudaSuccess)
+            counted_malloc_host(&sl.h_err, sizeof(uint32_t)) != cudaSuccess)
             rc = fail(RADIK_ERR_CUDA, "server slot set-up failed");
         if (rc == RADIK_OK) rc = radik_ws_create(1, 1, 4, &sl.ws);
         if (rc != RADIK_OK) {
@@ -344,7 +368,19 @@ int radik_server_get_stats(radik_server* sv, radik_server_stats* out) {
     for (double x : l) sum += x;
     out->mean_us = l.empty() ? 0.0 : sum / static_cast<double>(l.size());
     out->mem_in_flight = static_cast<int64_t>(sv->in_flight);
-    out->mem_pool = static_cast<int64_t>(server_pool_bytes(sv));
+    out->mem_pool = static_cast<int64_t>(sv->pool_bytes);
+    return RADIK_OK;
+}
+
+int radik_server_get_latencies(radik_server* sv, uint64_t* tickets, double* lat_us, int64_t cap, int64_t* n) {
+    if (!sv || !n || cap < 0 || (cap > 0 && (!tickets || !lat_us))) return fail(RADIK_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    const int64_t have = static_cast<int64_t>(sv->lat_us.size());
+    for (int64_t i = 0; i < std::min(cap, have); ++i) {
+        tickets[i] = sv->lat_ticket[i];
+        lat_us[i] = sv->lat_us[i];
+    }
+    *n = have;
     return RADIK_OK;
 }
 
@@ -355,6 +391,7 @@ int radik_server_reset_stats(radik_server* sv) {
     sv->submitted = 0;
     sv->elements = 0;
     sv->lat_us.clear();
+    sv->lat_ticket.clear();
     return RADIK_OK;
 }
 

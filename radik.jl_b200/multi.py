@@ -18,6 +18,8 @@ default; the tests pass the CPU restatement.
 """
 from __future__ import annotations
 
+import importlib
+import sys
 from typing import Callable, Sequence
 
 import numpy as np
@@ -50,9 +52,25 @@ def split_task(n: int, world: int) -> list[tuple[int, int]]:
     return out
 
 
+def _engine():
+    """The engine package this module belongs to (loaded as its submodule)."""
+    pkg = __name__.rpartition(".")[0]
+    if not pkg or pkg not in sys.modules:
+        raise RuntimeError("multi.py must be imported as a submodule of the engine package "
+                           "(e.g. radik_b200.multi) to run the engine's top-k")
+    return importlib.import_module(pkg)
+
+
 def _engine_topk(values, task_lens, k, indices, largest, rev):
-    from . import topk  # deferred: the engine needs its library and a GPU
-    return topk(values, list(task_lens), k, indices=indices, largest=largest, rev=rev)
+    return _engine().topk(values, list(task_lens), k, indices=indices, largest=largest, rev=rev)
+
+
+def _world_rank(group):
+    """(world size, rank); an uninitialised process group is one rank."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return 1, 0
+    return dist.get_world_size(group), dist.get_rank(group)
 
 
 def merge_candidates(values, positions, k: int, *, largest: bool, rev: bool, topk_fn: Callable):
@@ -85,11 +103,14 @@ def distributed_topk_single(local_values, start: int, k: int, *, largest: bool =
     lv, li = fn(local_values, [n], k, pos, largest, rev)
     lv = lv.reshape(-1)[:k].contiguous()
     li = li.reshape(-1)[:k].to(torch.int64).contiguous()
-    world = dist.get_world_size(group)
-    gv = [torch.empty_like(lv) for _ in range(world)]
-    gi = [torch.empty_like(li) for _ in range(world)]
-    dist.all_gather(gv, lv, group=group)
-    dist.all_gather(gi, li, group=group)
+    world, _ = _world_rank(group)
+    if world == 1:
+        gv, gi = [lv], [li]
+    else:
+        gv = [torch.empty_like(lv) for _ in range(world)]
+        gi = [torch.empty_like(li) for _ in range(world)]
+        dist.all_gather(gv, lv, group=group)
+        dist.all_gather(gi, li, group=group)
     v, i = merge_candidates(torch.cat(gv), torch.cat(gi), k, largest=largest, rev=rev, topk_fn=fn)
     v = v.reshape(-1)
     i = i.reshape(-1).to(torch.int64)
@@ -99,27 +120,38 @@ def distributed_topk_single(local_values, start: int, k: int, *, largest: bool =
     return v, i
 
 
+def local_shard(task_lens: Sequence[int], world: int, rank: int) -> tuple[int, int, int, int]:
+    """This rank's task range [t0, t1) of shard_tasks and the element range
+    [lo, hi) those tasks occupy in the concatenated batch."""
+    t0, t1 = shard_tasks(task_lens, world)[rank]
+    offs = np.concatenate([[0], np.cumsum(np.asarray(task_lens, dtype=np.int64))])
+    return t0, t1, int(offs[t0]), int(offs[t1])
+
+
 def distributed_topk_batch(values, task_lens: Sequence[int], k: int, *, largest: bool = True, rev: bool = False,
-                           topk_fn: Callable | None = None, group=None, gather: bool = False):
+                           topk_fn: Callable | None = None, group=None, gather: bool = False,
+                           local: bool = False):
     """Batched top k with the tasks sharded across ranks (no collective on
     the data path).  `values` holds the whole concatenated batch on every
-    rank (or at least this rank's tasks at their global offsets).  Returns
-    this rank's task range and its rows; with gather=True every rank also
-    receives all rows (one all_gather_object, for checking)."""
+    rank, or -- with local=True -- only this rank's tasks (its local_shard,
+    from offset 0).  Returns this rank's task range and its rows; with
+    gather=True every rank also receives all rows (one all_gather_object,
+    for checking)."""
     import torch.distributed as dist
     fn = topk_fn or _engine_topk
-    world = dist.get_world_size(group)
-    rank = dist.get_rank(group)
-    ranges = shard_tasks(task_lens, world)
-    t0, t1 = ranges[rank]
-    offs = np.concatenate([[0], np.cumsum(np.asarray(task_lens, dtype=np.int64))])
-    lo, hi = int(offs[t0]), int(offs[t1])
+    world, rank = _world_rank(group)
+    t0, t1, lo, hi = local_shard(task_lens, world, rank)
+    if local:
+        lo, hi = 0, hi - lo
+    lens = [int(x) for x in task_lens[t0:t1]]
     if t1 > t0:
-        v, i = fn(values[lo:hi], list(task_lens[t0:t1]), k, None, largest, rev)
+        v, i = fn(values[lo:hi], lens, k, None, largest, rev)
     else:
         v, i = None, None
     if not gather:
         return (t0, t1), (v, i)
+    if world == 1:
+        return (t0, t1), [((t0, t1), None if v is None else (v.cpu(), i.cpu()))]
     parts = [None] * world
     dist.all_gather_object(parts, ((t0, t1), None if v is None else (v.cpu(), i.cpu())), group=group)
     return (t0, t1), parts

@@ -223,8 +223,7 @@ KERNEL_FORMS = [
     {"RADIK_WS": "1", "RADIK_WST": "256", "RADIK_WSJ": "8", "RADIK_WSS": "16"},
     {"RADIK_WS": "1", "RADIK_WST": "256", "RADIK_WSJ": "4", "RADIK_WSS": "24"},
     {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "8"},
-    {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "12", "RADIK_WS_SAMPLE": "4096",
-     "RADIK_WS_WINDOWS": "3"},
+    {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "12", "RADIK_WS_SAMPLE": "4096"},
     {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "8", "RADIK_DEFER": "1"},
 ]
 

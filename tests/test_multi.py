@@ -20,10 +20,15 @@ ROOT = pathlib.Path(__file__).resolve().parents[1]
 
 
 def _load_multi():
-    spec = importlib.util.spec_from_file_location("radik_b200_multi", ROOT / "radik.jl_b200" / "multi.py")
-    mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
-    return mod
+    """multi.py as the engine package's submodule, the way users import it
+    (its engine top-k resolves through the package)."""
+    if "radik_b200" not in sys.modules:
+        spec = importlib.util.spec_from_file_location("radik_b200", ROOT / "radik.jl_b200" / "__init__.py",
+                                                      submodule_search_locations=[str(ROOT / "radik.jl_b200")])
+        pkg = importlib.util.module_from_spec(spec)
+        sys.modules["radik_b200"] = pkg
+        spec.loader.exec_module(pkg)
+    return importlib.import_module("radik_b200.multi")
 
 
 def _load_oracle():
@@ -101,6 +106,20 @@ def test_shard_and_split_geometry():
         assert sl[0][0] == 0 and sl[-1][1] == 10_003
         assert all(a[1] == b[0] for a, b in zip(sl, sl[1:]))
         assert all(s[0] % 4 == 0 for s in sl)
+        for r in range(world):
+            t0, t1, lo, hi = multi.local_shard(lens, world, r)
+            assert (t0, t1) == ranges[r] and lo == sum(lens[:t0]) and hi == sum(lens[:t1])
+
+
+def test_engine_topk_needs_the_package():
+    """Loaded on its own, outside the package, the module refuses to guess
+    where the engine is."""
+    spec = importlib.util.spec_from_file_location("lone_multi", ROOT / "radik.jl_b200" / "multi.py")
+    lone = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(lone)
+    with pytest.raises(RuntimeError, match="submodule of the engine package"):
+        lone._engine_topk(torch.zeros(4), [4], 1, None, True, False)
+    assert _load_multi()._engine().__name__ == "radik_b200"
 
 
 @pytest.mark.parametrize("k,largest,rev", [(1, True, False), (100, True, False), (257, False, True)])
