@@ -197,6 +197,16 @@ int radik_server_get_stats(radik_server* server, radik_server_stats* stats);
  * (submission to completion) for i < min(cap, *n); *n receives how many
  * there are.  Callers group them by request shape. */
 int radik_server_get_latencies(radik_server* server, uint64_t* tickets, double* lat_us, int64_t cap, int64_t* n);
+/* One launched batch: its k, rows (tasks), longest row, input elements, the
+ * device time of its work on the slot's stream (plan upload to the last
+ * kernel) and the host time the worker spent launching it. */
+typedef struct radik_server_batch {
+    int64_t k, rows, max_row_len;
+    double elements, gpu_us, launch_us;
+} radik_server_batch;
+/* The batches completed since the last reset, in completion order:
+ * out[i] for i < min(cap, *n); *n receives how many there are. */
+int radik_server_get_batches(radik_server* server, radik_server_batch* out, int64_t cap, int64_t* n);
 int radik_server_reset_stats(radik_server* server);
 
 /* ---- Stage entry points: the reference kernels' own contracts ----------- */

@@ -475,6 +475,18 @@ class Server:
         check(L.radik_server_get_latencies(self._h, tk, lat, cap, ctypes.byref(n)))
         return {int(tk[i]): float(lat[i]) for i in range(min(cap, int(n.value)))}
 
+    def batches(self) -> list[dict]:
+        """The launched batches completed since the last reset_stats: k,
+        rows, longest row, elements, device time and host launch time (us)."""
+        from ._lib import ServerBatch
+        L = load()
+        n = ctypes.c_int64()
+        check(L.radik_server_get_batches(self._h, None, 0, ctypes.byref(n)))
+        cap = int(n.value)
+        arr = (ServerBatch * max(cap, 1))()
+        check(L.radik_server_get_batches(self._h, arr, cap, ctypes.byref(n)))
+        return [{f: getattr(arr[i], f) for f, _ in ServerBatch._fields_} for i in range(min(cap, int(n.value)))]
+
     def reset_stats(self) -> None:
         check(load().radik_server_reset_stats(self._h))
 

@@ -34,7 +34,7 @@ EXPORTS = (
     "radik_count_bin_ex", "radik_count_bin", "radik_select_bin", "radik_filter",
     "radik_last_error", "radik_status_string", "radik_version", "radik_alloc_count",
     "radik_server_create", "radik_server_destroy", "radik_server_submit", "radik_server_wait",
-    "radik_server_get_stats", "radik_server_get_latencies", "radik_server_reset_stats",
+    "radik_server_get_stats", "radik_server_get_latencies", "radik_server_get_batches", "radik_server_reset_stats",
 )
 
 
@@ -57,6 +57,12 @@ class ServerStats(ctypes.Structure):
                 ("rows", ctypes.c_uint64), ("elements", ctypes.c_double), ("p50_us", ctypes.c_double),
                 ("p99_us", ctypes.c_double), ("mean_us", ctypes.c_double), ("mem_in_flight", ctypes.c_int64),
                 ("mem_pool", ctypes.c_int64)]
+
+
+class ServerBatch(ctypes.Structure):
+    """radik_server_batch (include/radik.h)."""
+    _fields_ = [("k", ctypes.c_int64), ("rows", ctypes.c_int64), ("max_row_len", ctypes.c_int64),
+                ("elements", ctypes.c_double), ("gpu_us", ctypes.c_double), ("launch_us", ctypes.c_double)]
 
 
 class RadiKError(Exception):
@@ -97,6 +103,7 @@ def _declare(L: ctypes.CDLL) -> None:
     L.radik_server_get_stats.argtypes = [P, ctypes.POINTER(ServerStats)]
     L.radik_server_get_latencies.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
                                              I64, ctypes.POINTER(I64)]
+    L.radik_server_get_batches.argtypes = [P, ctypes.POINTER(ServerBatch), I64, ctypes.POINTER(I64)]
     L.radik_server_reset_stats.argtypes = [P]
     L.radik_alloc_count.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
     L.radik_last_error.restype = ctypes.c_char_p

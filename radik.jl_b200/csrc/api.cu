@@ -55,10 +55,14 @@ cudaError_t counted_malloc_host(T** p, size_t n) {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
-    cudaError_t ensure(size_t b) {
+    // Grows to at least b bytes; `grow` > 1 allocates that much more, so a
+    // buffer that keeps growing (the request server's) reallocates -- and
+    // synchronises the device -- only rarely.
+    cudaError_t ensure(size_t b, double grow = 1.0) {
         if (b <= bytes) return cudaSuccess;
         if (p) { cudaFree(p); p = nullptr; bytes = 0; }
         size_t nb = b < 256 ? 256 : b;
+        if (grow > 1.0) nb = std::max(nb, static_cast<size_t>(static_cast<double>(nb) * grow));
         cudaError_t e = counted_malloc(&p, nb);
         if (e == cudaSuccess) bytes = nb;
         return e;
@@ -241,6 +245,7 @@ struct radik_ws {
     int64_t n = 0;          // longest task served (RadiKWorkspace n)
     int64_t num_tasks = 0;  // largest batch (RadiKWorkspace num_tasks)
     int index_bytes = 4;
+    double grow = 1.0;          // device buffers grow by this factor over a call's need (the server's: 1.5)
     cudaStream_t last_stream = nullptr;
     uint32_t* h_err = nullptr;  // pinned
     char* h_stage = nullptr;    // pinned staging of plan descriptors (stream-ordered uploads)
@@ -354,10 +359,19 @@ void segment_tasks(Plan& np, const int64_t* lens, int64_t T, int64_t k, uint32_t
             const int64_t S = njobs * nchunks * kSampleChunk;
             const int64_t stride = (td.len / (njobs * nchunks)) & ~int64_t(3);
             const double lam = static_cast<double>(kk) * static_cast<double>(S) / static_cast<double>(td.len);
-            // Rank of the threshold among the sample's group maxima: lam + 3 sqrt(lam) + 6
-            // keeps the chance that fewer than k elements lie above it negligible.
-            const int64_t r = static_cast<int64_t>(std::ceil(lam + 3.0 * std::sqrt(lam) + 6.0));
-            if (allow_sample && nseg * static_cast<int64_t>(kk) >= 8192 && stride >= kSampleChunk + 4 && r <= 64) {
+            // Rank of the threshold among the sample's group maxima: the
+            // threshold is too high only when r or more sampled elements lie
+            // above the task's k-th, a Poisson(lam) tail; lam + max(3 sqrt(lam)
+            // + 6, 5 sqrt(lam)) keeps it below about 1e-5 for small lam and
+            // 5 sigma for large lam (a large k on long rows: a served batch
+            // holds hundreds of such tasks, each failure a recomputation).  Each
+            // sampling block keeps its top r of its 1024 maxima and the last
+            // one ranks the union in shared memory: r <= 256 and njobs * r <=
+            // 8192.
+            const double margin = std::max(3.0 * std::sqrt(lam) + 6.0, 5.0 * std::sqrt(lam));
+            const int64_t r = static_cast<int64_t>(std::ceil(lam + margin));
+            const bool r_fits = r <= 256 && njobs * r <= 8192;
+            if (allow_sample && nseg * static_cast<int64_t>(kk) >= 8192 && stride >= kSampleChunk + 4 && r_fits) {
                 td.flags |= kTaskSampled;
                 for (int64_t j = 0; j < njobs; ++j) {
                     SampleJob sj;
@@ -454,7 +468,14 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     // memory).  In the warp-specialised form, sampled split tasks run in
     // flush mode and need no candidate buffer of k entries, so a batch made
     // only of them gets the minimum buffer.  RADIK_WS=0/1 forces a form.
-    const uint32_t cap_bar = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(bar_threads) * bar_vec, bar_threads));
+    uint32_t cap_bar = static_cast<uint32_t>(fused_cap(kk, static_cast<size_t>(bar_threads) * bar_vec, bar_threads));
+    if (kk > kBitonicMax) {
+        // Room for the radix sort's second key buffer and digit counters in
+        // shared memory too (finish_task); such a block has an SM to itself
+        // either way.
+        const size_t want = round_up(2 * kk + (static_cast<size_t>(bar_threads) / 32 * 256 + 256) / 2 + 64, 64);
+        if (fused_smem(want, bar_threads, bar_vec) <= smem_max) cap_bar = std::max<uint32_t>(cap_bar, want);
+    }
     const uint32_t cap_ws = static_cast<uint32_t>(
         fused_cap(all_flush ? 0 : kk, static_cast<size_t>(ws_threads) * ws_j, ws_threads));
     {
@@ -617,15 +638,16 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
     // Device buffers.
     const StateLayout L(T);
     const size_t desc_bytes = plan_desc_bytes(np);
-    cudaError_t e = ws->state.ensure(L.bytes);
-    if (e == cudaSuccess) e = ws->desc.ensure(desc_bytes);
+    const double g = ws->grow;
+    cudaError_t e = ws->state.ensure(L.bytes, g);
+    if (e == cudaSuccess) e = ws->desc.ensure(desc_bytes, g);
     if (e == cudaSuccess && np.fused) {
-        e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.cand_entries));
-        if (e == cudaSuccess) e = ws->samples.ensure(sizeof(uint64_t) * static_cast<size_t>(np.sample_entries));
+        e = ws->cand.ensure(sizeof(uint64_t) * static_cast<size_t>(np.cand_entries), g);
+        if (e == cudaSuccess) e = ws->samples.ensure(sizeof(uint64_t) * static_cast<size_t>(np.sample_entries), g);
         const size_t sort_blocks = std::max<size_t>(
             {static_cast<size_t>(np.grid), static_cast<size_t>(np.retry_grid), np.merge_tasks.size()});
         if (e == cudaSuccess && kk > kBitonicMax)
-            e = ws->scratch.ensure(sizeof(uint64_t) * sort_blocks * kk);
+            e = ws->scratch.ensure(sizeof(uint64_t) * sort_blocks * kk, g);
     }
     if (e == cudaSuccess && !np.fused) {
         e = ws->hist.ensure(sizeof(uint32_t) * 4096 * static_cast<size_t>(T));
@@ -647,8 +669,10 @@ int build_plan(radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t
             if (ws->h_stage) cudaFreeHost(ws->h_stage);
             ws->h_stage = nullptr;
             ws->h_stage_bytes = 0;
-            e = counted_malloc_host(&ws->h_stage, desc_bytes);
-            if (e == cudaSuccess) ws->h_stage_bytes = desc_bytes;
+            const size_t nb = ws->grow > 1.0 ? static_cast<size_t>(static_cast<double>(desc_bytes) * ws->grow)
+                                             : desc_bytes;
+            e = counted_malloc_host(&ws->h_stage, nb);
+            if (e == cudaSuccess) ws->h_stage_bytes = nb;
         }
         if (e == cudaSuccess) {
             if (T) std::memcpy(ws->h_stage + np.tasks_off, np.tasks.data(), sizeof(FusedTask) * T);

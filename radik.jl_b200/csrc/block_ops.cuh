@@ -625,63 +625,77 @@ __device__ __forceinline__ void bitonic_sort_u64(uint64_t* a, uint32_t n, bool d
 // Stable ascending LSD radix sort (8-bit digits) of a[0, n) using b[0, n) as
 // scratch; digits on which all keys agree are skipped.  Returns the buffer
 // (a or b) that holds the sorted keys.  Buffers may live in shared or global
-// memory (generic addressing).
+// memory (generic addressing).  Every warp owns a contiguous chunk of the
+// keys; a digit pass is: per-warp histograms of the chunk, the digit-major
+// exclusive scan over (digit, warp) -- each warp's first slot per digit --
+// and a scatter in which every warp walks its chunk in order, 32 keys at a
+// time, ranking lanes of equal digits with one match: no block barrier
+// inside the scatter, five per pass.
 template <int THREADS>
 __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, uint32_t n, BlockScratch<THREADS>& s,
                                     uint32_t* warp_digit /* [THREADS/32][256] shared */,
                                     uint32_t* digit_base /* [256] shared */) {
     constexpr int W = THREADS / 32;
     const int tid = threadIdx.x, w = tid >> 5;
+    const uint32_t lane = lane_id();
     uint64_t vor = 0, vand = ~0ull;
     for (uint32_t i = tid; i < n; i += THREADS) { vor |= a[i]; vand &= a[i]; }
     block_or_and<THREADS>(vor, vand, s);
     const uint64_t diff = vor ^ vand;
+    const uint32_t chunk = (n + W - 1) / W;
+    const uint32_t lo = static_cast<uint32_t>(w) * chunk < n ? static_cast<uint32_t>(w) * chunk : n;
+    const uint32_t hi = lo + chunk < n ? lo + chunk : n;
+    uint32_t* mine = warp_digit + w * 256;
     for (int sh = 0; sh < 64; sh += 8) {
         if (((diff >> sh) & 0xffull) == 0) continue;
-        // digit histogram -> exclusive offsets
-        for (int i = tid; i < 256; i += THREADS) s.hist[i] = 0;
+        // 1. histogram of this warp's chunk
+        for (uint32_t j = lane; j < 256; j += 32) mine[j] = 0;
+        __syncwarp();
+        for (uint32_t base = lo; base < hi; base += 32) {
+            const uint32_t i = base + lane;
+            warp_hist_add(mine, i < hi ? static_cast<uint32_t>((a[i] >> sh) & 0xff) : 0u, i < hi);
+        }
         block_sync<THREADS>();
-        for (uint32_t base = 0; base < n; base += THREADS) {
-            const uint32_t i = base + tid;
-            warp_hist_add(s.hist, i < n ? static_cast<uint32_t>((a[i] >> sh) & 0xff) : 0u, i < n);
+        // 2. digit totals, their exclusive scan, then each warp's first slot
+        for (int d = tid; d < 256; d += THREADS) {
+            uint32_t tot = 0;
+            for (int ww = 0; ww < W; ++ww) tot += warp_digit[ww * 256 + d];
+            digit_base[d] = tot;
         }
         block_sync<THREADS>();
         if (tid < 32) {
             uint32_t c[8], sum = 0;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) { c[j] = s.hist[tid * 8 + j]; sum += c[j]; }
-            uint32_t inc = warp_inclusive_scan<true>(sum);
-            uint32_t run = inc - sum;
+            for (int j = 0; j < 8; ++j) { c[j] = digit_base[tid * 8 + j]; sum += c[j]; }
+            uint32_t run = warp_inclusive_scan<true>(sum) - sum;
 #pragma unroll
             for (int j = 0; j < 8; ++j) { digit_base[tid * 8 + j] = run; run += c[j]; }
         }
         block_sync<THREADS>();
-        // stable scatter, one tile of THREADS keys at a time in order
-        for (uint32_t base = 0; base < n; base += THREADS) {
-            uint32_t i = base + tid;
-            bool valid = i < n;
-            uint64_t v = valid ? a[i] : 0ull;
-            uint32_t d = valid ? static_cast<uint32_t>((v >> sh) & 0xff) : 256u + lane_id();
-            uint32_t peers = __match_any_sync(kFullMask, d);
-            uint32_t rank = __popc(peers & lanemask_lt());
-            for (int j = tid; j < W * 256; j += THREADS) warp_digit[j] = 0;
-            block_sync<THREADS>();
-            if (valid && rank == 0) warp_digit[w * 256 + d] = __popc(peers);
-            block_sync<THREADS>();
-            // per digit: prefix over warps (thread d handles digit d)
-            for (int dd = tid; dd < 256; dd += THREADS) {
-                uint32_t run = digit_base[dd];
-                for (int ww = 0; ww < W; ++ww) {
-                    uint32_t c = warp_digit[ww * 256 + dd];
-                    warp_digit[ww * 256 + dd] = run;
-                    run += c;
-                }
-                digit_base[dd] = run;
+        for (int d = tid; d < 256; d += THREADS) {
+            uint32_t run = digit_base[d];
+            for (int ww = 0; ww < W; ++ww) {
+                const uint32_t c = warp_digit[ww * 256 + d];
+                warp_digit[ww * 256 + d] = run;
+                run += c;
             }
-            block_sync<THREADS>();
-            if (valid) b[warp_digit[w * 256 + d] + rank] = v;
-            block_sync<THREADS>();
         }
+        block_sync<THREADS>();
+        // 3. stable scatter: chunks in warp order, keys in order inside a chunk
+        for (uint32_t base = lo; base < hi; base += 32) {
+            const uint32_t i = base + lane;
+            const bool valid = i < hi;
+            const uint64_t v = valid ? a[i] : 0ull;
+            const uint32_t d = valid ? static_cast<uint32_t>((v >> sh) & 0xff) : 256u + lane;
+            const uint32_t peers = __match_any_sync(kFullMask, d);
+            const uint32_t below = peers & lanemask_lt();
+            const uint32_t off = valid ? mine[d] : 0u;
+            if (valid) b[off + __popc(below)] = v;
+            __syncwarp();
+            if (valid && below == 0u) mine[d] = off + __popc(peers);  // the first lane of each digit advances it
+            __syncwarp();
+        }
+        block_sync<THREADS>();
         uint64_t* t = a; a = b; b = t;
     }
     return a;

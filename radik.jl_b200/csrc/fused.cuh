@@ -262,9 +262,14 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
         block_sync<THREADS>();
         bitonic_sort_u64<THREADS>(buf, P);
     } else {
-        uint64_t* scratch = p.sort_scratch + static_cast<int64_t>(blockIdx.x) * p.kmax;
+        // Digit counters behind the keys; the second key buffer in shared
+        // memory too when the buffer holds it (the merge kernel's does),
+        // else the block's slice of the global sort scratch.
         uint32_t* wd = reinterpret_cast<uint32_t*>(buf + m);
         uint32_t* db = wd + (THREADS / 32) * 256;
+        const size_t soff = (static_cast<size_t>(m) + ((THREADS / 32) * 256 + 256) / 2 + 2) & ~size_t(1);
+        uint64_t* scratch = (soff + m <= p.cap) ? buf + soff
+                                                : p.sort_scratch + static_cast<int64_t>(blockIdx.x) * p.kmax;
         sorted = radix_sort_u64<THREADS>(buf, scratch, m, sh.bs, wd, db);
     }
     block_sync<THREADS>();
@@ -337,29 +342,34 @@ __device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint
     for (uint32_t i = tid; i < cnt; i += THREADS) atomicAdd(hist + (static_cast<uint32_t>(buf[i] >> shift) & bmask), 1u);
     block_sync<THREADS>();
     if (tid < 32) {
-        // Bins from the top: lane l takes bins nb-1-l*per ... (per <= 8).
-        const uint32_t lane = tid, per = (nb + 31u) / 32u;
-        uint32_t sum = 0;
-        for (uint32_t j = 0; j < per; ++j) {
-            const uint32_t rb = lane * per + j;
-            sum += rb < nb ? hist[nb - 1u - rb] : 0u;
+        // Bins from the top: lane l takes bins nb-1-8l ... nb-8-8l (all
+        // loads at once; bins past nb count 0).
+        const uint32_t lane = tid;
+        uint32_t h[8], sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t rb = lane * 8u + static_cast<uint32_t>(j);
+            h[j] = rb < nb ? hist[nb - 1u - rb] : 0u;
+            sum += h[j];
         }
         const uint32_t incl = warp_inclusive_scan<true>(sum);
         uint32_t run = incl - sum;  // entries in the bins above this lane's
         uint32_t bstar = 0xffffffffu, need = 0, big = 0;
-        for (uint32_t j = 0; j < per; ++j) {
-            const uint32_t rb = lane * per + j;
-            if (rb >= nb) break;
-            const uint32_t b = nb - 1u - rb, h = hist[b];
-            off[b] = run;
-            if (run < m) {  // a bin that holds some of the m best
-                big = h > big ? h : big;
-                if (run + h >= m) {
-                    bstar = b;
-                    need = m - run;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t rb = lane * 8u + static_cast<uint32_t>(j);
+            if (rb < nb) {
+                const uint32_t b = nb - 1u - rb;
+                off[b] = run;
+                if (run < m) {  // a bin that holds some of the m best
+                    big = h[j] > big ? h[j] : big;
+                    if (run + h[j] >= m) {
+                        bstar = b;
+                        need = m - run;
+                    }
                 }
             }
-            run += h;
+            run += h[j];
         }
         big = __reduce_max_sync(kFullMask, big);
         const uint32_t who = __ballot_sync(kFullMask, bstar != 0xffffffffu);

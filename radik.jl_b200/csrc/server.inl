@@ -40,6 +40,8 @@ struct ServerReq {
 struct ServerSlot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done_ev = nullptr;
+    cudaEvent_t t0_ev = nullptr, t1_ev = nullptr;  // the batch's device work, timed
+    radik_server_batch info{};                     // the batch in flight (k, rows, elements, launch time)
     radik_ws* ws = nullptr;
     DevBuf io;                  // FusedTaskIO per row of the batch
     FusedTaskIO* h_io = nullptr;  // pinned staging
@@ -68,6 +70,7 @@ struct radik_server {
     double elements = 0;
     std::vector<double> lat_us;
     std::vector<uint64_t> lat_ticket;  // ticket of lat_us[i]
+    std::vector<radik_server_batch> batch_log;  // completed batches since the last reset
     std::string worker_error;
     size_t pool_bytes = 0;  // device bytes of the slots' workspaces, updated by the worker under mu
 };
@@ -100,8 +103,9 @@ int server_launch(ServerSlot& sl, const std::vector<ServerReq>& batch) {
         if (sl.h_io) cudaFreeHost(sl.h_io);
         sl.h_io = nullptr;
         sl.h_io_cap = 0;
-        RADIK_CUDA(counted_malloc_host(&sl.h_io, sizeof(FusedTaskIO) * T));
-        sl.h_io_cap = static_cast<size_t>(T);
+        const size_t cap = static_cast<size_t>(T) + static_cast<size_t>(T) / 2;  // headroom: reallocate rarely
+        RADIK_CUDA(counted_malloc_host(&sl.h_io, sizeof(FusedTaskIO) * cap));
+        sl.h_io_cap = cap;
     }
     int64_t row = 0;
     for (const ServerReq& r : batch) {
@@ -117,17 +121,24 @@ int server_launch(ServerSlot& sl, const std::vector<ServerReq>& batch) {
     radik_ws* ws = sl.ws;
     ws->num_tasks = std::max<int64_t>(ws->num_tasks, T);
     ws->n = std::max<int64_t>(ws->n, maxlen);
+    sl.info.k = r0.k;
+    sl.info.rows = T;
+    sl.info.max_row_len = maxlen;
+    sl.info.elements = 0;
+    for (const ServerReq& r : batch) sl.info.elements += static_cast<double>(r.rows) * static_cast<double>(r.row_len);
     const uint32_t flags = r0.flags | RADIK_ASYNC;
+    RADIK_CUDA(cudaEventRecord(sl.t0_ev, sl.stream));
     int rc = build_plan(ws, lens.data(), T, r0.k, flags, r0.idx_bytes, sl.stream, true);
     if (rc) return rc;
     if (!ws->plan.fused) return fail(RADIK_ERR_INVALID, "request shape has no fused plan (k too large to serve)");
-    if (sl.io.ensure(sizeof(FusedTaskIO) * T) != cudaSuccess) return fail(RADIK_ERR_OOM, "server io table");
+    if (sl.io.ensure(sizeof(FusedTaskIO) * T, 1.5) != cudaSuccess) return fail(RADIK_ERR_OOM, "server io table");
     RADIK_CUDA(cudaMemcpyAsync(sl.io.p, sl.h_io, sizeof(FusedTaskIO) * T, cudaMemcpyHostToDevice, sl.stream));
     RADIK_CUDA(cudaMemsetAsync(err_ptr(ws), 0, 4, sl.stream));
     FusedParams p = fused_params(ws, nullptr, nullptr, r0.idx_bytes, nullptr, nullptr, r0.k, flags);
     p.task_io = sl.io.as<FusedTaskIO>();
     rc = run_fused(ws, p, flags, sl.stream);
     if (rc) return rc;
+    RADIK_CUDA(cudaEventRecord(sl.t1_ev, sl.stream));
     RADIK_CUDA(cudaMemcpyAsync(sl.h_err, err_ptr(ws), 4, cudaMemcpyDeviceToHost, sl.stream));
     RADIK_CUDA(cudaEventRecord(sl.done_ev, sl.stream));
     return RADIK_OK;
@@ -156,6 +167,12 @@ void server_worker(radik_server* sv) {
                 sv->elements += static_cast<double>(r.rows) * static_cast<double>(r.row_len);
                 sv->lat_us.push_back(std::chrono::duration<double, std::micro>(r.t_done - r.t_submit).count());
                 sv->lat_ticket.push_back(id);
+            }
+            if (q == cudaSuccess) {
+                float ms = 0.0f;
+                if (cudaEventElapsedTime(&ms, sl.t0_ev, sl.t1_ev) != cudaSuccess) cudaGetLastError();
+                sl.info.gpu_us = 1e3 * static_cast<double>(ms);
+                sv->batch_log.push_back(sl.info);
             }
             sv->in_flight -= sl.mem;
             sl.mem = 0;
@@ -200,7 +217,9 @@ void server_worker(radik_server* sv) {
             sl.mem = mem;
             sv->in_flight += mem;
             lk.unlock();
+            const auto l0 = ServerClock::now();
             const int rc = server_launch(sl, batch);
+            sl.info.launch_us = std::chrono::duration<double, std::micro>(ServerClock::now() - l0).count();
             std::string err;
             if (rc != RADIK_OK) {
                 err = g_last_error;
@@ -265,9 +284,11 @@ int radik_server_create(const radik_server_config* cfg, radik_server** out) {
         int rc = RADIK_OK;
         if (cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl.done_ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&sl.t0_ev) != cudaSuccess || cudaEventCreate(&sl.t1_ev) != cudaSuccess ||
             counted_malloc_host(&sl.h_err, sizeof(uint32_t)) != cudaSuccess)
             rc = fail(RADIK_ERR_CUDA, "server slot set-up failed");
         if (rc == RADIK_OK) rc = radik_ws_create(1, 1, 4, &sl.ws);
+        if (rc == RADIK_OK) sl.ws->grow = 1.5;  // batches vary: grow with headroom, reallocate rarely
         if (rc != RADIK_OK) {
             radik_server_destroy(sv);
             return rc;
@@ -294,6 +315,8 @@ int radik_server_destroy(radik_server* sv) {
         if (sl.h_io) cudaFreeHost(sl.h_io);
         if (sl.h_err) cudaFreeHost(sl.h_err);
         if (sl.done_ev) cudaEventDestroy(sl.done_ev);
+        if (sl.t0_ev) cudaEventDestroy(sl.t0_ev);
+        if (sl.t1_ev) cudaEventDestroy(sl.t1_ev);
         if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     delete sv;
@@ -384,6 +407,15 @@ int radik_server_get_latencies(radik_server* sv, uint64_t* tickets, double* lat_
     return RADIK_OK;
 }
 
+int radik_server_get_batches(radik_server* sv, radik_server_batch* out, int64_t cap, int64_t* n) {
+    if (!sv || !n || cap < 0 || (cap > 0 && !out)) return fail(RADIK_ERR_INVALID, "NULL argument");
+    std::lock_guard<std::mutex> lk(sv->mu);
+    const int64_t have = static_cast<int64_t>(sv->batch_log.size());
+    for (int64_t i = 0; i < std::min(cap, have); ++i) out[i] = sv->batch_log[i];
+    *n = have;
+    return RADIK_OK;
+}
+
 int radik_server_reset_stats(radik_server* sv) {
     if (!sv) return fail(RADIK_ERR_INVALID, "NULL argument");
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -392,6 +424,7 @@ int radik_server_reset_stats(radik_server* sv) {
     sv->elements = 0;
     sv->lat_us.clear();
     sv->lat_ticket.clear();
+    sv->batch_log.clear();
     return RADIK_OK;
 }
 

@@ -81,6 +81,7 @@ def test_server_results_in_the_mix_equal_alone(radik, oracle, torch_cuda):
         for d, k, lg, rv, _ in reqs:
             solo.append(srv.wait(srv.submit(d, k, largest=lg, rev=rv), timeout_s=60))
         st = srv.stats()
+        log = srv.batches()
     for a, w, m, s in zip(alone, want, mixed, solo):
         _same_as_oracle(m, w)
         _same_as_oracle(s, w)
@@ -88,6 +89,11 @@ def test_server_results_in_the_mix_equal_alone(radik, oracle, torch_cuda):
         _same(s, a)
     assert st["completed"] == 2 * len(reqs)
     assert st["batches"] < 2 * len(reqs)  # requests were packed together
+    # the batch log: one entry per launched batch, rows and elements adding up to the requests'
+    assert len(log) == st["batches"]
+    assert sum(b["rows"] for b in log) == 2 * sum(r[0].shape[0] for r in reqs)
+    assert sum(b["elements"] for b in log) == 2 * sum(r[0].numel() for r in reqs)
+    assert all(b["gpu_us"] > 0 and b["launch_us"] > 0 and b["k"] in (1, 50, 1024) for b in log)
     assert 0 < st["p50_us"] <= st["p99_us"]
 
 

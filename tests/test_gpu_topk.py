@@ -321,8 +321,9 @@ def test_short_segments_single_task(oracle, radik, torch_cuda, monkeypatch, k):
     """The autotuner's short-segment plan (RADIK_SEG_MIN=4: 8192-element
     segments) on the 2^20-element N(0,1) task of seed 0: 128 segments, with a
     sampled threshold and the merge kernel where the segments' candidates
-    would be many (128 k >= 8192) and the sample's rank allows it (k <= 1000
-    here), else unsampled with every segment's k candidates."""
+    would be many (128 k >= 8192) and the sample's rank fits (8 sampling
+    blocks of 4096 elements: lam = k / 32, r = lam + max(3 sqrt(lam) + 6,
+    5 sqrt(lam)) <= 256), else unsampled with every segment's k candidates."""
     monkeypatch.setenv("RADIK_SEG_MIN", "4")
     n = 1 << 20
     x = np.random.default_rng(0).standard_normal(n).astype(np.float32)
@@ -331,7 +332,9 @@ def test_short_segments_single_task(oracle, radik, torch_cuda, monkeypatch, k):
     info = ws.plan_info()
     ws.close()
     assert info["segments"] == 128
-    assert (info["sample_jobs"] > 0) == (64 <= k <= 1000)
+    lam = k * 8 * 8 * 512 / n
+    r = int(np.ceil(lam + max(3 * np.sqrt(lam) + 6, 5 * np.sqrt(lam))))
+    assert (info["sample_jobs"] > 0) == (128 * k >= 8192 and r <= 256)
     _compare(oracle, radik, torch_cuda, x, [n], k)
     _compare(oracle, radik, torch_cuda, x, [n], k, largest=False, rev=True)
     q = np.round(x * 32.0).astype(np.float32) / 32.0  # ties at the k-th value
