@@ -396,14 +396,15 @@ def run_ours(args, rank: int, world: int, dist, config: str | None = None, *, e2
     torch.cuda.synchronize()
     clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    per = []
+    # Per-step events made before the timed region: creating them inside it
+    # costs host time that would show as gaps between the steps.
+    per = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     ev0.record(stream)
     for i in range(args.steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a, b = per[i]
         a.record(stream)
         step(i)
         b.record(stream)
-        per.append((a, b))
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier()

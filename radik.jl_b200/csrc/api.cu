@@ -125,6 +125,7 @@ FusedKernel pick_fused_ws(int threads, int j, int stages, bool scale) {
     if (threads == 256 && j == 4 && stages == 24) return scale ? fused_ws_ptr<8, 4, 24, true>() : fused_ws_ptr<8, 4, 24, false>();
     if (threads == 128 && j == 8 && stages == 8) return scale ? fused_ws_ptr<4, 8, 8, true>() : fused_ws_ptr<4, 8, 8, false>();
     if (threads == 128 && j == 8 && stages == 12) return scale ? fused_ws_ptr<4, 8, 12, true>() : fused_ws_ptr<4, 8, 12, false>();
+    if (threads == 64 && j == 8 && stages == 4) return scale ? fused_ws_ptr<2, 8, 4, true>() : fused_ws_ptr<2, 8, 4, false>();
     return nullptr;
 }
 
@@ -297,10 +298,10 @@ uint32_t* err_ptr(radik_ws* ws) { return ws->state.as<uint32_t>(StateLayout::kEr
 // k entries plus the slack of a mid-stream shrink, followed by the per-warp
 // candidate regions (kRegionEntries).  Candidates that find no room are
 // re-offered after a shrink, so no region needs to hold a whole tile.
-size_t fused_cap(size_t k, size_t tile, int threads) {
+size_t fused_cap(size_t k, size_t tile, int threads, size_t regions = kRegionEntries) {
     (void)tile;
     size_t cap_s = round_up(k + std::max<size_t>(k / 4, 512), 64);
-    size_t cap = cap_s + kRegionEntries;
+    size_t cap = cap_s + regions;
     size_t p2 = 1;
     while (p2 < std::min<size_t>(k, kBitonicMax)) p2 <<= 1;
     cap = std::max(cap, p2);
@@ -319,7 +320,7 @@ int64_t pick_seg_len(int64_t N, int64_t resident, size_t tile, bool fused, int s
         seg_len = std::max<int64_t>(static_cast<int64_t>(min_tiles) * static_cast<int64_t>(tile), target);
     }
     seg_len = static_cast<int64_t>(round_up(static_cast<size_t>(seg_len), tile));
-    if (!fused) seg_len = std::max<int64_t>(seg_len, 1 << 20);
+    if (!fused) seg_len = std::max<int64_t>(seg_len, 1 << 16);
     return seg_len;
 }
 
@@ -354,8 +355,17 @@ void segment_tasks(Plan& np, const int64_t* lens, int64_t T, int64_t k, uint32_t
             np.cand_entries += nseg * static_cast<int64_t>(kk);
             // Seed the global threshold from a sample when the segments' own
             // k-th values would leave a large merge (many segments, large k).
-            const int64_t njobs = std::min<int64_t>(128, std::max<int64_t>(8, td.len >> 21));
-            const int64_t nchunks = 8;
+            // Sampling blocks and chunks per block: fewer of them when k is a
+            // large share of the task, so that lam (and the rank r below) stays
+            // within what a block ranks.
+            int64_t njobs = std::min<int64_t>(128, std::max<int64_t>(8, td.len >> 21));
+            int64_t nchunks = 8;
+            auto lam_of = [&](int64_t jobs, int64_t ch) {
+                return static_cast<double>(kk) * static_cast<double>(jobs * ch * kSampleChunk) /
+                       static_cast<double>(td.len);
+            };
+            while (njobs > 1 && lam_of(njobs, nchunks) > 160.0) njobs = std::max<int64_t>(1, njobs / 2);
+            while (nchunks > 1 && lam_of(njobs, nchunks) > 160.0) nchunks /= 2;
             const int64_t S = njobs * nchunks * kSampleChunk;
             const int64_t stride = (td.len / (njobs * nchunks)) & ~int64_t(3);
             const double lam = static_cast<double>(kk) * static_cast<double>(S) / static_cast<double>(td.len);
@@ -366,11 +376,11 @@ void segment_tasks(Plan& np, const int64_t* lens, int64_t T, int64_t k, uint32_t
             // 5 sigma for large lam (a large k on long rows: a served batch
             // holds hundreds of such tasks, each failure a recomputation).  Each
             // sampling block keeps its top r of its 1024 maxima and the last
-            // one ranks the union in shared memory: r <= 256 and njobs * r <=
-            // 8192.
+            // one ranks the union in shared memory: r <= 256, at most a quarter
+            // of a block's maxima, and njobs * r <= 8192.
             const double margin = std::max(3.0 * std::sqrt(lam) + 6.0, 5.0 * std::sqrt(lam));
             const int64_t r = static_cast<int64_t>(std::ceil(lam + margin));
-            const bool r_fits = r <= 256 && njobs * r <= 8192;
+            const bool r_fits = r <= 256 && r <= nchunks * (kSampleChunk / 4) / 4 && njobs * r <= 8192;
             if (allow_sample && nseg * static_cast<int64_t>(kk) >= 8192 && stride >= kSampleChunk + 4 && r_fits) {
                 td.flags |= kTaskSampled;
                 for (int64_t j = 0; j < njobs; ++j) {
@@ -476,13 +486,14 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
         const size_t want = round_up(2 * kk + (static_cast<size_t>(bar_threads) / 32 * 256 + 256) / 2 + 64, 64);
         if (fused_smem(want, bar_threads, bar_vec) <= smem_max) cap_bar = std::max<uint32_t>(cap_bar, want);
     }
-    const uint32_t cap_ws = static_cast<uint32_t>(
-        fused_cap(all_flush ? 0 : kk, static_cast<size_t>(ws_threads) * ws_j, ws_threads));
+    const uint32_t cap_ws = static_cast<uint32_t>(fused_cap(all_flush ? 0 : kk, static_cast<size_t>(ws_threads) * ws_j,
+                                                            ws_threads, ws_region_entries(ws_threads / 32)));
     {
         const size_t sm_bytes = static_cast<size_t>(di.max_smem_optin) + 1024;  // per SM, a block's reserve included
         const size_t ws_blk = fused_ws_smem(cap_ws, ws_j, np.ws_stages) + 2048;
         const size_t bar_blk = fused_smem(cap_bar, bar_threads, bar_vec) + 2048;
-        const size_t ws_occ = std::min<size_t>(4, sm_bytes / ws_blk), bar_occ = std::min<size_t>(3, sm_bytes / bar_blk);
+        const size_t ws_occ = std::min<size_t>(static_cast<size_t>(ws_blocks_per_sm(ws_threads / 32)), sm_bytes / ws_blk),
+                     bar_occ = std::min<size_t>(3, sm_bytes / bar_blk);
         const size_t ws_ring = static_cast<size_t>(np.ws_stages) * 128 * ws_j * 4;
         const size_t bar_ring = static_cast<size_t>(kStages) * bar_threads * bar_vec * 4;
         const bool ws_auto = ws_occ >= 3 || (ws_occ >= 1 && ws_occ * ws_ring >= bar_occ * bar_ring);
@@ -1151,6 +1162,9 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     { TuneConfig c = d; c.form = 1; c.ws_stages = 12; cands.push_back(c); }
     { TuneConfig c = d; c.form = 1; c.ws_threads = 256; c.ws_stages = 16; cands.push_back(c); }
     { TuneConfig c = d; c.form = 1; c.sample_max = 4096; cands.push_back(c); }
+    // The narrow form: 2 consumer warps, 7 blocks per SM -- one round for a
+    // batch of up to 7 tasks per SM.
+    { TuneConfig c = d; c.form = 1; c.ws_threads = 64; c.ws_stages = 4; cands.push_back(c); }
     { TuneConfig c = d; c.form = 0; cands.push_back(c); }
     { TuneConfig c = d; c.seg_div = 2; cands.push_back(c); }
     { TuneConfig c = d; c.seg_div = 6; cands.push_back(c); }

@@ -122,10 +122,12 @@ __device__ __forceinline__ bool ws_warp_wait(uint64_t* bar, uint32_t parity, uin
 constexpr uint32_t kSampleChunkLen = 64;
 constexpr uint32_t kSampleMax = 4096;
 
-// Sampled elements of a task (0: no sample); the same in producer and consumers.
-__device__ __forceinline__ uint32_t ws_sample_len(const FusedParams& p, const FusedTask& td) {
+// Sampled elements of a task (0: no sample); the same in producer and
+// consumers.  `most`: the sample tiles the block's consumer warps can take
+// (one each), in elements.
+__device__ __forceinline__ uint32_t ws_sample_len(const FusedParams& p, const FusedTask& td, uint32_t most) {
     if (p.retry || td.nseg != 1) return 0u;
-    const uint32_t smax = p.sample_max;
+    const uint32_t smax = p.sample_max < most ? p.sample_max : most;
     if (td.len >= 16 * static_cast<int64_t>(smax)) return smax;
     if (td.len >= 4 * static_cast<int64_t>(smax)) return smax / 2;
     return 0u;
@@ -170,7 +172,7 @@ __device__ void ws_producer(const FusedParams& p, float* ring, uint64_t* full, u
         const SegGeom G = seg_geom<TW, kScale>(p, w, &tv);
         if (G.skip) continue;
         bool ok = true;
-        const uint32_t slen = ws_sample_len(p, G.td);
+        const uint32_t slen = ws_sample_len(p, G.td, static_cast<uint32_t>(THREADS / 32) * TW);
         const uint32_t ns = ws_sample_rank(G.td, slen) != 0 ? slen / TW : 0u;
         const uint32_t nch = slen / kSampleChunkLen;
         const uint32_t nt = G.ntiles + ns;
@@ -300,13 +302,22 @@ __device__ __forceinline__ uint32_t ws_place(const float4* src, uint32_t elems, 
     return om;
 }
 
+// Candidate append regions of the warp-specialised form, all consumer warps
+// together: the narrow form (2 consumer warps, 7 blocks per SM) has half.
+__host__ __device__ constexpr uint32_t ws_region_entries(int ncw) {
+    return ncw == 2 ? kRegionEntries / 2 : kRegionEntries;
+}
+// Blocks per SM the form is compiled for (its register budget).
+__host__ __device__ constexpr int ws_blocks_per_sm(int ncw) { return ncw == 2 ? 7 : (ncw >= 8 ? 3 : 4); }
+
 template <int NCW, int J, int STAGES, bool kScale>
-__global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_kernel(FusedParams p) {
+__global__ void __launch_bounds__((NCW + 1) * 32, ws_blocks_per_sm(NCW)) fused_ws_kernel(FusedParams p) {
     grid_dep_wait();  // launched after the previous kernel of the call (state clear or sampler)
     constexpr int THREADS = NCW * 32;             // consumer threads
     constexpr uint32_t TW = 128u * J;             // elements per warp tile (one ring stage)
     constexpr uint32_t TW4 = TW / 4;              // float4 per warp tile
-    constexpr uint32_t R = kRegionEntries / NCW;  // append region of each consumer warp
+    constexpr uint32_t REG = ws_region_entries(NCW);
+    constexpr uint32_t R = REG / NCW;  // append region of each consumer warp
     static_assert(J * 4 <= 32, "element bits of a lane fit in 32 bits");
     // Ring tile g sits in stage g % STAGES and belongs to warp g % NCW.  With
     // STAGES a multiple of NCW every stage belongs to one warp, so the tile a
@@ -316,8 +327,9 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
     // stages a warp could wait on phase n while phase n - 1, another warp's
     // tile, was still in flight, and the parity test would pass at once.)
     static_assert(STAGES % NCW == 0, "every ring stage belongs to one consumer warp");
-    static_assert(kSampleMax / TW <= static_cast<uint32_t>(NCW), "every sample tile has its own warp");
-    static_assert(kSampleMax / 4 <= kRegionEntries, "group maxima fit in the candidate buffer");
+    // ws_sample_len keeps the sample to one tile per consumer warp; its group
+    // maxima (redo path) fit in the candidate buffer.
+    static_assert(static_cast<uint32_t>(NCW) * TW / 4 <= REG, "group maxima fit in the candidate buffer");
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ WsShared<THREADS> sh;
     float* ring = reinterpret_cast<float*>(smem_raw);
@@ -354,7 +366,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
     // ---- consumer warps ----------------------------------------------------
     const uint32_t lt = lanemask_lt();
     const uint32_t cap = p.cap;
-    const uint32_t cap_s = p.cap - kRegionEntries;  // settled region [0, cap_s), then the warp regions
+    const uint32_t cap_s = p.cap - REG;  // settled region [0, cap_s), then the warp regions
     uint64_t* region = s_buf + cap_s + warp * R;
     const uint32_t compact_at = cap - max(cap / 8, static_cast<uint32_t>(THREADS) + 8u);
     const float4* ring4 = reinterpret_cast<const float4*>(ring);
@@ -388,7 +400,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, (NCW >= 8 ? 3 : 4)) fused_ws_k
             const uint32_t pos0 = static_cast<uint32_t>(G.a0);
             const uint32_t nvec = static_cast<uint32_t>(G.nvec);
             const uint32_t ntiles = G.ntiles;
-            const uint32_t slen = ws_sample_len(p, td);
+            const uint32_t slen = ws_sample_len(p, td, static_cast<uint32_t>(NCW) * TW);
             const uint32_t sample_r = ws_sample_rank(td, slen);
             const uint32_t ns = sample_r != 0 ? slen / TW : 0u;
             const float4* gsrc = reinterpret_cast<const float4*>(tv.data + G.a0);

@@ -61,10 +61,18 @@ __global__ void __launch_bounds__(THREADS) plain_hist_input(PlainParams p) {
         for (int i = threadIdx.x; i < 4096; i += THREADS) h[i] = 0;
         __syncthreads();
         const float scaler = kScale ? task_scaler(p.data, td.start, td.len, 1) : 0.0f;
-        for (int64_t i = threadIdx.x; i < sg.len; i += THREADS) {
-            uint32_t bits = __float_as_uint(p.data[td.start + sg.pos + i]);
-            uint32_t s = score_of<kScale>(bits, scaler, p.sp);
-            atomicAdd(&h[s >> 20], 1u);
+        const float* src = p.data + td.start + sg.pos;
+        // Four independent loads per thread in flight, then their bins.
+        for (int64_t i0 = 0; i0 < sg.len; i0 += 4 * THREADS) {
+            uint32_t bits[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t i = i0 + u * THREADS + threadIdx.x;
+                bits[u] = i < sg.len ? __float_as_uint(src[i]) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (i0 + u * THREADS + threadIdx.x < sg.len) atomicAdd(&h[score_of<kScale>(bits[u], scaler, p.sp) >> 20], 1u);
         }
         __syncthreads();
         uint32_t* gh = p.hist + static_cast<int64_t>(sg.task) * 4096;
@@ -148,18 +156,28 @@ __global__ void __launch_bounds__(THREADS) plain_compact_input(PlainParams p) {
         const uint32_t bin = copy_all ? 0u : p.st[t].bin;
         const bool allwin = copy_all ? true : (p.st[t].allwin != 0);
         uint32_t* nnext = &p.st[t].nnext;
-        for (int64_t i = threadIdx.x; i < sg.len; i += THREADS) {
-            const int64_t g = td.start + sg.pos + i;
-            uint32_t bits = __float_as_uint(p.data[g]);
-            uint32_t s = score_of<kScale>(bits, scaler, p.sp);
-            uint64_t c = make_composite(s, static_cast<uint32_t>(g - td.start));
-            uint32_t d = s >> 20;
-            if (copy_all || d > bin || (d == bin && allwin)) {
-                emit_winner(p, t, c);
-            } else if (d == bin) {
-                uint32_t slot = atomicAdd(nnext, 1u);
-                if (slot < static_cast<uint32_t>(td.len)) p.cand[0][td.start + slot] = c;
-                else record_error(p.err, kErrCapacity);
+        // Four independent loads per thread in flight, then their tests.
+        for (int64_t i0 = 0; i0 < sg.len; i0 += 4 * THREADS) {
+            uint32_t bits[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t i = i0 + u * THREADS + threadIdx.x;
+                bits[u] = i < sg.len ? __float_as_uint(p.data[td.start + sg.pos + i]) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int64_t i = i0 + u * THREADS + threadIdx.x;
+                if (i >= sg.len) continue;
+                const uint32_t s = score_of<kScale>(bits[u], scaler, p.sp);
+                const uint64_t c = make_composite(s, static_cast<uint32_t>(sg.pos + i));
+                const uint32_t d = s >> 20;
+                if (copy_all || d > bin || (d == bin && allwin)) {
+                    emit_winner(p, t, c);
+                } else if (d == bin) {
+                    uint32_t slot = atomicAdd(nnext, 1u);
+                    if (slot < static_cast<uint32_t>(td.len)) p.cand[0][td.start + slot] = c;
+                    else record_error(p.err, kErrCapacity);
+                }
             }
         }
     }

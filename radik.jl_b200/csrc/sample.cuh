@@ -27,7 +27,7 @@ struct SampleJob {
     int32_t job_in_task;
     int32_t njobs;       // CTAs sampling this task
     int32_t r;           // sample rank (from the best) of the threshold, <= 256 (njobs * r <= 8192)
-    int32_t nchunks;     // chunks per CTA (a multiple of THREADS * 16 / kSampleChunk)
+    int32_t nchunks;     // chunks per CTA (1 to 8)
     int32_t pad_;
     int64_t pos0;        // position (inside the task) of this CTA's first chunk
     int64_t stride;      // distance between consecutive chunks (a multiple of 4)

@@ -225,11 +225,12 @@ KERNEL_FORMS = [
     {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "8"},
     {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "12", "RADIK_WS_SAMPLE": "4096"},
     {"RADIK_WS": "1", "RADIK_WST": "128", "RADIK_WSJ": "8", "RADIK_WSS": "8", "RADIK_DEFER": "1"},
+    {"RADIK_WS": "1", "RADIK_WST": "64", "RADIK_WSJ": "8", "RADIK_WSS": "4"},
 ]
 
 
 @pytest.mark.parametrize("form", KERNEL_FORMS, ids=["barrier", "ws-256-j8", "ws-256-j4", "ws-128-s8", "ws-128-s12",
-                                                    "ws-128-s8-defer"])
+                                                    "ws-128-s8-defer", "ws-64-s4-narrow"])
 def test_many_items_per_block(oracle, radik, torch_cuda, monkeypatch, form):
     """A grid of 2-3 blocks works through every batch, so each block takes
     many work items in a row: ring stages, phases and item slots carry over
