@@ -539,7 +539,14 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
         for (int64_t t = 0; t < T; ++t)
             if (np.tasks[t].flags & kTaskSampled) {
                 np.tasks[t].flags |= kTaskFlush;
-                np.merge_tasks.push_back(static_cast<int32_t>(t));
+                // A small k is finished by the block that flushes the task's
+                // last segment (one histogram pass over a few hundred
+                // candidates); a large k goes to the merge and rank kernels,
+                // which spread its k^2 placement over the GPU.
+                if (kk <= kBucketMaxK && env_int("RADIK_FINISH_HERE", 1) != 0)
+                    np.tasks[t].flags |= kTaskFinishHere;
+                else
+                    np.merge_tasks.push_back(static_cast<int32_t>(t));
             }
     // Deferred finish: when a batch has at least as many single-segment
     // tasks as resident blocks, their blocks leave the candidates in a

@@ -42,7 +42,11 @@ namespace radik {
 // candidates in the task's region (p.cap entries) and queues it, so that the
 // block moves on to its next task at once; blocks with no streaming left
 // finish queued tasks (fused_ws.cuh).
-enum : uint32_t { kTaskLargest = 1u, kTaskAscend = 2u, kTaskSampled = 4u, kTaskFlush = 8u, kTaskDefer = 16u };
+// kTaskFinishHere: a flush-mode task with a small k that the block flushing
+// its last segment finishes (no merge kernel).
+enum : uint32_t {
+    kTaskLargest = 1u, kTaskAscend = 2u, kTaskSampled = 4u, kTaskFlush = 8u, kTaskDefer = 16u, kTaskFinishHere = 32u
+};
 
 struct FusedTask {
     int64_t start;   // global offset of the task in p.data (uniform-input mode)

@@ -629,7 +629,57 @@ __global__ void __launch_bounds__((NCW + 1) * 32, ws_blocks_per_sm(NCW)) fused_w
             }
             gbase += ns + ntiles;  // the ring tiles of this item (the redo reads global memory)
 
-            if (flush) {
+            if (flush && (td.flags & kTaskFinishHere) != 0u) {
+                // The block that flushes a task's last segment finishes it:
+                // the region, filtered by the task's threshold (kept within
+                // the buffer by shrinks), then the k best, sorted and written.
+                __threadfence();  // this block's region writes before its arrival
+                block_sync<THREADS>();
+                if (tid == 0) {
+                    const uint32_t done = atomicAdd(p.task_done + t, 1u);
+                    sh.f.last = (done == static_cast<uint32_t>(td.nseg - 1)) ? 1u : 0u;
+                }
+                block_sync<THREADS>();
+                if (sh.f.last) {
+                    __threadfence();
+                    if (tid == 0) {
+                        sh.f.cnt = 0;
+                        sh.f.gthr = load_volatile_u64(p.gthr + t);
+                        sh.f.base = __ldcg(p.task_cnt + t);
+                    }
+                    block_sync<THREADS>();
+                    const uint64_t gt = sh.f.gthr;
+                    const uint32_t cregion = static_cast<uint32_t>(td.nseg) * p.kmax;
+                    // A count above the region means a flush overflowed it and
+                    // already flagged the task for the retry launch.
+                    const uint32_t n = sh.f.base <= cregion ? sh.f.base : 0u;
+                    const unsigned long long* csrc = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
+                    for (uint32_t b0 = 0; b0 < n; b0 += THREADS) {
+                        {
+                            const uint32_t ii = b0 + tid;
+                            const uint64_t c = (ii < n) ? __ldcg(csrc + ii) : 0ull;
+                            warp_append((ii < n) && c > gt, c, s_buf, &sh.f.cnt, cap, p.err);
+                        }
+                        block_sync<THREADS>();
+                        const uint32_t cnt_now = sh.f.cnt;
+                        block_sync<THREADS>();
+                        if (cnt_now > compact_at) shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh.f);
+                    }
+                    block_sync<THREADS>();
+                    const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
+                    if (sh.f.base > cregion) {
+                    } else if (sh.f.cnt < want) {
+                        // The sampled threshold was above the task's k-th
+                        // composite: the retry launch recomputes the task.
+                        if (tid == 0) {
+                            p.fail[t] = 1u;
+                            atomicExch(p.fail_any, 1u);
+                        }
+                    } else {
+                        finish_candidates<THREADS, kScale>(p, tv, s_buf, sh.f);
+                    }
+                }
+            } else if (flush) {
                 // merge.cuh selects the task's k best from its candidate region.
             } else if (!multi && (td.flags & kTaskDefer) != 0u && !p.retry && p.defer_q != nullptr) {
                 // Deferred finish: the candidates (at least min(len, k), all in
