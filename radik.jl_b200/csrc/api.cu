@@ -236,6 +236,8 @@ struct Plan {
     std::vector<FusedTask> tasks;
     std::vector<FusedSeg> segs;
     std::vector<SampleJob> jobs;
+    // One sampling block per task (sample_one_kernel), every job's whole sample in it.
+    bool sample_one = false;
     std::vector<int32_t> merge_tasks;
     // Deferred single-segment tasks (finished by blocks with no streaming left).
     std::vector<int32_t> defer_tasks;
@@ -409,6 +411,29 @@ void segment_tasks(Plan& np, const int64_t* lens, int64_t T, int64_t k, uint32_t
             np.segs.push_back(sg);
         }
         off += td.len;
+    }
+    // When every sampled task's sample fits one block, one block per task
+    // reads and ranks it (no sample buffer, no merge between blocks).
+    np.sample_one = false;
+    if (!np.jobs.empty() && env_int("RADIK_SAMPLE_ONE", 1) != 0) {
+        bool fits = true;
+        for (const SampleJob& sj : np.jobs)
+            fits = fits && static_cast<int64_t>(sj.njobs) * sj.nchunks <= kSampleOneMaxChunks;
+        if (fits) {
+            std::vector<SampleJob> one;
+            for (const SampleJob& sj : np.jobs)
+                if (sj.job_in_task == 0) {
+                    SampleJob o1 = sj;
+                    o1.nchunks = sj.njobs * sj.nchunks;
+                    o1.njobs = 1;
+                    o1.pos0 = 0;
+                    o1.out_base = 0;
+                    one.push_back(o1);
+                }
+            np.jobs.swap(one);
+            np.sample_entries = 0;
+            np.sample_one = true;
+        }
     }
     // Longest work first (uneven batches), stable on task order.
     std::stable_sort(np.segs.begin(), np.segs.end(),
@@ -778,6 +803,8 @@ bool rank_pays(size_t ntasks, uint64_t k) {
 // Clears the per-call state (n 32-bit words): a kernel rather than a memset,
 // so that the call's first kernel can be launched programmatically after it.
 __global__ void state_clear_kernel(uint32_t* p, uint32_t n) {
+    grid_dep_wait();  // the stream's previous kernel (a previous call's) may still read the state
+    grid_dep_launch();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = 0u;
 }
 
@@ -809,15 +836,21 @@ int run_fused(radik_ws* ws, const FusedParams& p, uint32_t flags, cudaStream_t s
     {
         const uint32_t nw = static_cast<uint32_t>((L.bytes - StateLayout::kWork) / 4);
         const unsigned cg = std::max(1u, std::min(148u * 4u, (nw + 255u) / 256u));
-        state_clear_kernel<<<cg, 256, 0, s>>>(ws->state.as<uint32_t>(StateLayout::kWork), nw);
-        RADIK_CUDA(cudaGetLastError());
+        RADIK_CUDA(launch_after(true, state_clear_kernel, dim3(cg), dim3(256), 0, s,
+                                ws->state.as<uint32_t>(StateLayout::kWork), nw));
     }
     if (!pl.jobs.empty()) {
-        SampleKernel sk = pick_sample(scale);
-        const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
-        RADIK_CUDA(launch_after(true, sk, dim3(static_cast<unsigned>(pl.jobs.size())), dim3(256), ssmem, s, p,
-                                static_cast<const SampleJob*>(ws->desc.as<SampleJob>(pl.jobs_off)),
-                                ws->samples.as<uint64_t>(), ws->state.as<uint32_t>(L.sdone)));
+        if (pl.sample_one) {
+            RADIK_CUDA(launch_after(true, scale ? sample_one_kernel<true> : sample_one_kernel<false>,
+                                    dim3(static_cast<unsigned>(pl.jobs.size())), dim3(kSampleOneThreads), 0, s, p,
+                                    static_cast<const SampleJob*>(ws->desc.as<SampleJob>(pl.jobs_off))));
+        } else {
+            SampleKernel sk = pick_sample(scale);
+            const size_t ssmem = sizeof(uint64_t) * std::max<size_t>(8 * kSampleChunk, 128 * 64);
+            RADIK_CUDA(launch_after(true, sk, dim3(static_cast<unsigned>(pl.jobs.size())), dim3(256), ssmem, s, p,
+                                    static_cast<const SampleJob*>(ws->desc.as<SampleJob>(pl.jobs_off)),
+                                    ws->samples.as<uint64_t>(), ws->state.as<uint32_t>(L.sdone)));
+        }
     }
     FusedKernel fk = pl.ws_form ? pick_fused_ws(pl.threads, pl.vec, pl.ws_stages, scale)
                                 : pick_fused(pl.threads, pl.vec, scale);

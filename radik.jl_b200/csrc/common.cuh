@@ -175,6 +175,11 @@ __device__ __forceinline__ bool block_sync_or(bool pred) {
 // stream finishes; it waits here before it reads anything that kernel wrote.
 // Without the attribute this returns at once.
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the stream's next kernel (launched programmatically) be scheduled now:
+// its blocks take free SM slots and wait in grid_dep_wait, which still waits
+// for this whole grid to complete and its writes to be visible.  Called once
+// all of a grid's blocks are resident, it hides the next launch's latency.
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 __device__ __forceinline__ void record_error(uint32_t* err, uint32_t bits) {
     if (err) atomicOr(err, bits);

@@ -309,8 +309,8 @@ constexpr uint32_t kBucketScanMax = 64;
 template <int THREADS>
 __device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint64_t* buf, uint32_t cnt, uint32_t want,
                                   FusedShared<THREADS>& sh) {
-    constexpr uint32_t Q = (kBucketMaxK + kBucketScanMax + THREADS - 1) / THREADS;  // bucket entries per thread
-    const uint32_t tid = threadIdx.x;
+    constexpr int NW = THREADS / 32;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const uint32_t m = cnt < want ? cnt : want;
     // Scratch behind the candidates: the buckets, then bucket offsets and
     // scatter cursors (256 words each).
@@ -322,13 +322,38 @@ __device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint
     uint32_t* cur = off + 256;
     uint32_t* hist = sh.bs.hist;
 
-    uint64_t vor = 0, vand = ~0ull;
-    for (uint32_t i = tid; i < cnt; i += THREADS) {
-        const uint64_t c = buf[i];
-        vor |= c;
-        vand &= c;
+    // OR and AND of the high and low words (one warp reduction each); the
+    // bins and cursors are cleared before the same barrier.
+    {
+        uint32_t hor = 0u, hand = ~0u, lor = 0u, land = ~0u;
+#pragma unroll 1
+        for (uint32_t i = tid; i < cnt; i += THREADS) {
+            const uint64_t c = buf[i];
+            hor |= static_cast<uint32_t>(c >> 32);
+            hand &= static_cast<uint32_t>(c >> 32);
+            lor |= static_cast<uint32_t>(c);
+            land &= static_cast<uint32_t>(c);
+        }
+        hor = __reduce_or_sync(kFullMask, hor);
+        hand = __reduce_and_sync(kFullMask, hand);
+        lor = __reduce_or_sync(kFullMask, lor);
+        land = __reduce_and_sync(kFullMask, land);
+        if (lane == 0) {
+            sh.bs.warp_a[warp] = (static_cast<uint64_t>(hor) << 32) | lor;
+            sh.bs.warp_b[warp] = (static_cast<uint64_t>(hand) << 32) | land;
+        }
+        for (uint32_t b = tid; b < 256u; b += THREADS) {
+            hist[b] = 0;
+            cur[b] = 0;
+        }
     }
-    block_or_and<THREADS>(vor, vand, sh.bs);
+    block_sync<THREADS>();
+    uint64_t vor = 0, vand = ~0ull;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        vor |= sh.bs.warp_a[w];
+        vand &= sh.bs.warp_b[w];
+    }
     const uint64_t diff = vor ^ vand;
     const int top = diff ? 63 - __clzll(static_cast<long long>(diff)) : 0;
     // Bins cut the scores only (a run of equal scores stays in one bin) unless
@@ -338,17 +363,12 @@ __device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint
     const int w = one_score ? (top + 1 < 8 ? top + 1 : 8) : (top - 31 < 8 ? top - 31 : 8);
     const int shift = top + 1 - w;
     const uint32_t nb = 1u << w, bmask = nb - 1u;
-    for (uint32_t b = tid; b < nb; b += THREADS) {
-        hist[b] = 0;
-        cur[b] = 0;
-    }
-    block_sync<THREADS>();
+#pragma unroll 1
     for (uint32_t i = tid; i < cnt; i += THREADS) atomicAdd(hist + (static_cast<uint32_t>(buf[i] >> shift) & bmask), 1u);
     block_sync<THREADS>();
-    if (tid < 32) {
+    if (warp == 0) {
         // Bins from the top: lane l takes bins nb-1-8l ... nb-8-8l (all
         // loads at once; bins past nb count 0).
-        const uint32_t lane = tid;
         uint32_t h[8], sum = 0;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
@@ -393,6 +413,7 @@ __device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint
     if (sh.bs.bc32[2] != 0u) return false;  // uniform; buf[0, cnt) is untouched
     const uint32_t nsel = bstar == 0xffffffffu ? 0u : off[bstar] + hist[bstar];  // entries of bins >= b*
     if (nsel != 0u) {
+#pragma unroll 1
         for (uint32_t i = tid; i < cnt; i += THREADS) {
             const uint64_t c = buf[i];
             const uint32_t b = static_cast<uint32_t>(c >> shift) & bmask;
@@ -400,55 +421,14 @@ __device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint
         }
     }
     block_sync<THREADS>();
-    // Ranks inside the bins by composite (descending); the need-th of b*
-    // is the bound tau of the m best.
-    uint64_t ce[Q];
-    uint32_t rd[Q];
-#pragma unroll
-    for (int q = 0; q < static_cast<int>(Q); ++q) {
-        const uint32_t s = static_cast<uint32_t>(q) * THREADS + tid;
-        ce[q] = s < nsel ? bucket[s] : 0ull;
-        rd[q] = 0;
-        if (s < nsel) {
-            const uint32_t b = static_cast<uint32_t>(ce[q] >> shift) & bmask;
-            const uint32_t lo = off[b], hi = lo + hist[b];
-            for (uint32_t j = lo; j < hi; ++j) rd[q] += bucket[j] > ce[q] ? 1u : 0u;
-            if (b == bstar && rd[q] == need - 1u) sh.gthr = ce[q];
-        }
-    }
-    block_sync<THREADS>();
-    const uint64_t tau = sh.gthr;
     const bool same_order = one_score || (tv.sp.flip == 0u) != tv.ascend;
     const uint32_t nan_key = key_of_bits(tv.sp.nan_bits);
-#pragma unroll
-    for (int q = 0; q < static_cast<int>(Q); ++q) {
-        const uint32_t s = static_cast<uint32_t>(q) * THREADS + tid;
-        if (s >= nsel) continue;
-        const uint64_t c = ce[q];
-        const uint32_t b = static_cast<uint32_t>(c >> shift) & bmask;
-        if (b == bstar && c < tau) continue;  // below the m best
-        const uint32_t sel_b = b == bstar ? need : hist[b];
-        uint32_t o;
-        if (same_order) {
-            o = off[b] + rd[q];
-        } else {
-            // Ascending scores: the bins below this one come first, then this
-            // bin's selected entries by ascending (score, position).
-            const uint32_t lo = off[b], hi = lo + hist[b];
-            const uint32_t sc = static_cast<uint32_t>(c >> 32), pc = composite_pos(c);
-            uint32_t ra = 0;
-            for (uint32_t j = lo; j < hi; ++j) {
-                const uint64_t y = bucket[j];
-                const uint32_t sy = static_cast<uint32_t>(y >> 32);
-                const bool in = b != bstar || y >= tau;
-                ra += (in && (sy < sc || (sy == sc && composite_pos(y) < pc))) ? 1u : 0u;
-            }
-            o = m - off[b] - sel_b + ra;
-        }
+    // Writes the selected entry c to row slot o.
+    auto emit = [&](uint64_t c, uint32_t o) {
         uint32_t pos = composite_pos(c);
         if (pos >= static_cast<uint64_t>(tv.len) || o >= m) {  // never expected; keep accesses in bounds
             record_error(p.err, pos >= static_cast<uint64_t>(tv.len) ? kErrBounds : kErrInternal);
-            continue;
+            return;
         }
         const uint32_t key = static_cast<uint32_t>(c >> 32) ^ tv.sp.flip;
         const float val = (key == nan_key) ? tv.data[pos] : value_of_key(key);
@@ -462,6 +442,49 @@ __device__ bool finish_by_buckets(const FusedParams& p, const TaskView& tv, uint
         tv.vout[o] = val;
         if (p.idx_bytes == 8) static_cast<int64_t*>(tv.iout)[o] = idx;
         else static_cast<int32_t*>(tv.iout)[o] = static_cast<int32_t>(idx);
+    };
+    // Ranks inside the bins by composite (descending).  In composite order
+    // (same_order) an entry's row slot is its bin's offset plus that rank and
+    // b*'s entries are in when the rank is below need: written at once.
+    // Otherwise the need-th of b* is the bound tau of the m best, found first.
+    // (Loops kept rolled: this runs once per task and its code is fetched cold.)
+#pragma unroll 1
+    for (uint32_t s = tid; s < nsel; s += THREADS) {
+        const uint64_t c = bucket[s];
+        const uint32_t b = static_cast<uint32_t>(c >> shift) & bmask;
+        const uint32_t lo = off[b], hi = lo + hist[b];
+        uint32_t rd = 0;
+#pragma unroll 1
+        for (uint32_t j = lo; j < hi; ++j) rd += bucket[j] > c ? 1u : 0u;
+        if (same_order) {
+            if (b != bstar || rd < need) emit(c, off[b] + rd);
+        } else if (b == bstar && rd == need - 1u) {
+            sh.gthr = c;
+        }
+    }
+    if (!same_order) {
+        block_sync<THREADS>();
+        const uint64_t tau = sh.gthr;
+#pragma unroll 1
+        for (uint32_t s = tid; s < nsel; s += THREADS) {
+            const uint64_t c = bucket[s];
+            const uint32_t b = static_cast<uint32_t>(c >> shift) & bmask;
+            if (b == bstar && c < tau) continue;  // below the m best
+            const uint32_t sel_b = b == bstar ? need : hist[b];
+            // Ascending scores: the bins below this one come first, then this
+            // bin's selected entries by ascending (score, position).
+            const uint32_t lo = off[b], hi = lo + hist[b];
+            const uint32_t sc = static_cast<uint32_t>(c >> 32), pc = composite_pos(c);
+            uint32_t ra = 0;
+#pragma unroll 1
+            for (uint32_t j = lo; j < hi; ++j) {
+                const uint64_t y = bucket[j];
+                const uint32_t sy = static_cast<uint32_t>(y >> 32);
+                const bool in = b != bstar || y >= tau;
+                ra += (in && (sy < sc || (sy == sc && composite_pos(y) < pc))) ? 1u : 0u;
+            }
+            emit(c, m - off[b] - sel_b + ra);
+        }
     }
     if (cnt < want && tid == 0) record_error(p.err, kErrInternal);  // the caller redoes a short count
     for (uint32_t j = m + tid; j < tv.k; j += THREADS) {

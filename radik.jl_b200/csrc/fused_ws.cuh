@@ -313,6 +313,7 @@ __host__ __device__ constexpr int ws_blocks_per_sm(int ncw) { return ncw == 2 ? 
 template <int NCW, int J, int STAGES, bool kScale>
 __global__ void __launch_bounds__((NCW + 1) * 32, ws_blocks_per_sm(NCW)) fused_ws_kernel(FusedParams p) {
     grid_dep_wait();  // launched after the previous kernel of the call (state clear or sampler)
+    grid_dep_launch();  // every block of the grid is resident (grid <= resident blocks)
     constexpr int THREADS = NCW * 32;             // consumer threads
     constexpr uint32_t TW = 128u * J;             // elements per warp tile (one ring stage)
     constexpr uint32_t TW4 = TW / 4;              // float4 per warp tile
@@ -654,16 +655,35 @@ __global__ void __launch_bounds__((NCW + 1) * 32, ws_blocks_per_sm(NCW)) fused_w
                     // already flagged the task for the retry launch.
                     const uint32_t n = sh.f.base <= cregion ? sh.f.base : 0u;
                     const unsigned long long* csrc = reinterpret_cast<const unsigned long long*>(p.cand + td.cbase);
-                    for (uint32_t b0 = 0; b0 < n; b0 += THREADS) {
-                        {
-                            const uint32_t ii = b0 + tid;
-                            const uint64_t c = (ii < n) ? __ldcg(csrc + ii) : 0ull;
-                            warp_append((ii < n) && c > gt, c, s_buf, &sh.f.cnt, cap, p.err);
+                    if (n <= cap) {
+                        // The region fits the buffer: every load in flight at
+                        // once, no shrinking, no barrier between the loads.
+                        constexpr int U = 4;
+                        for (uint32_t b0 = 0; b0 < n; b0 += U * THREADS) {
+                            uint64_t c[U];
+#pragma unroll
+                            for (int u = 0; u < U; ++u) {
+                                const uint32_t ii = b0 + static_cast<uint32_t>(u) * THREADS + tid;
+                                c[u] = (ii < n) ? __ldcg(csrc + ii) : 0ull;
+                            }
+#pragma unroll
+                            for (int u = 0; u < U; ++u) {
+                                const uint32_t ii = b0 + static_cast<uint32_t>(u) * THREADS + tid;
+                                warp_append((ii < n) && c[u] > gt, c[u], s_buf, &sh.f.cnt, cap, p.err);
+                            }
                         }
-                        block_sync<THREADS>();
-                        const uint32_t cnt_now = sh.f.cnt;
-                        block_sync<THREADS>();
-                        if (cnt_now > compact_at) shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh.f);
+                    } else {
+                        for (uint32_t b0 = 0; b0 < n; b0 += THREADS) {
+                            {
+                                const uint32_t ii = b0 + tid;
+                                const uint64_t c = (ii < n) ? __ldcg(csrc + ii) : 0ull;
+                                warp_append((ii < n) && c > gt, c, s_buf, &sh.f.cnt, cap, p.err);
+                            }
+                            block_sync<THREADS>();
+                            const uint32_t cnt_now = sh.f.cnt;
+                            block_sync<THREADS>();
+                            if (cnt_now > compact_at) shrink_mid<THREADS>(p, k, mid_keep, s_buf, sh.f);
+                        }
                     }
                     block_sync<THREADS>();
                     const uint32_t want = tv.len < static_cast<int64_t>(k) ? static_cast<uint32_t>(tv.len) : k;
