@@ -1,7 +1,8 @@
 """Benchmark of the B200 exact Float32 radix top-k (one JSON line on rank 0).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config uniform_batch|adversarial_single|uneven_batch]
+                    [--config uniform_batch|adversarial_single|uneven_batch|single_1m|
+                              rows64_k8192|serving] [--tune-file PATH]
 
 A step is one batched top-k over the configuration's synthetic input (seeded,
 shapes and distributions of the workload; no dataset exists):
@@ -13,6 +14,9 @@ shapes and distributions of the workload; no dataset exists):
   uneven_batch        4096 tasks, lengths lognormal(median 20,000, sigma 1.5)
                       clamped to [1, 4,194,304] (seed 3), N(0,1), custom Int32
                       indices (a permutation), k=64, largest
+  single_1m           one task of 2^20 N(0,1) (seed 0), k=100, largest
+  rows64_k8192        64 tasks x 2^20 N(0,1), k=8192, largest (the serving
+                      stream's heaviest request shape)
   serving             the request server on a Poisson stream of top-k requests
                       (see run_serving)
 `value` is elements/s with the inputs already in HBM (timed with CUDA events
@@ -74,6 +78,9 @@ CONFIGS = {
     "uneven_batch": dict(k=64, largest=True, rev=False, custom_idx=True),
     # The reference's CPU-runnable case: one task of 2^20 N(0,1), seed 0.
     "single_1m": dict(k=100, largest=True, rev=False, custom_idx=False),
+    # The serving stream's heaviest request shape: 64 rows of 2^20 N(0,1),
+    # k = 8192 (sampled thresholds, the merge and rank kernels, radix sorts).
+    "rows64_k8192": dict(k=8192, largest=True, rev=False, custom_idx=False),
 }
 
 
@@ -84,6 +91,8 @@ def task_lens_of(name: str) -> list[int]:
         return [1 << 28]
     if name == "single_1m":
         return [1 << 20]
+    if name == "rows64_k8192":
+        return [1 << 20] * 64
     rng = np.random.default_rng(3)
     v = np.clip(np.round(rng.lognormal(np.log(20000), 1.5, size=4096)), 1, 4_194_304)
     return [int(x) for x in v]
@@ -221,6 +230,9 @@ def run_reference(args, rank: int, world: int):
     elif args.config == "single_1m":
         sample_lens = lens
         sample = "the whole 2^20-element task per step"
+    elif args.config == "rows64_k8192":
+        sample_lens = lens[:4]
+        sample = "4 of the 64 rows per step"
     else:
         sample_lens = lens[:256]
         sample = "the first 256 of the 4096 tasks per step"
@@ -290,6 +302,8 @@ def cpu_baseline_quick(args, config: str) -> dict:
         sl, sample = [1 << 22], "one 2^22-element task of the same mixture, 3 repetitions"
     elif config == "single_1m":
         sl, sample = lens, "the whole 2^20-element task, 3 repetitions"
+    elif config == "rows64_k8192":
+        sl, sample = lens[:4], "4 of the 64 rows, 3 repetitions"
     else:
         sl, sample = lens[:256], "first 256 of the 4096 tasks, 3 repetitions"
     N = int(sum(sl))
@@ -372,9 +386,19 @@ def run_ours(args, rank: int, world: int, dist, config: str | None = None, *, e2
     ws = radik.RadiKWorkspace("cuda", max(lens), T)
     stream = torch.cuda.current_stream()
     # Pick the fastest configuration for this batch shape (untimed set-up);
-    # it also prepares the plan.
-    tuned = ws.autotune(vo, io, xs[0], ind, lens, k, cfg["largest"], not cfg["rev"], False, ind is not None,
-                        reps=3, stream=stream)
+    # it also prepares the plan.  With --tune-file, a table saved by an
+    # earlier run decides instead (same plan under a profiler), or this run's
+    # choice is saved there.
+    main_run = config is None or config == args.config
+    tune_file = pathlib.Path(args.tune_file) if (getattr(args, "tune_file", None) and main_run) else None
+    if tune_file is not None and tune_file.exists():
+        radik.tune_load(tune_file)
+        tuned = {"ms": None, "loaded_from": str(tune_file)}
+    else:
+        tuned = ws.autotune(vo, io, xs[0], ind, lens, k, cfg["largest"], not cfg["rev"], False, ind is not None,
+                            reps=3, stream=stream)
+        if tune_file is not None and rank == 0:
+            radik.tune_save(tune_file)
 
     def step(i):
         radik.topk_radix_select_(vo, io, ws, xs[i % nbuf], ind, lens, k, cfg["largest"], not cfg["rev"],
@@ -715,6 +739,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="uniform_batch on one GPU without the adversarial_single and serving sub-blocks")
+    ap.add_argument("--tune-file", default=None,
+                    help="tuning table: loaded instead of autotuning when it exists, else written after it")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -88,16 +88,29 @@ typedef struct radik_plan_info {
 int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info);
 
 /* Autotuner (engine-specific, no reference counterpart): runs the call
- * below on the caller's data with each candidate configuration of the fused
- * path (kernel form, block and ring shape, sample size, segment size),
- * `reps` timed calls each, and keeps the fastest in ws for this batch shape
- * (task_lens, k, flags, index width); later calls with that shape use it.
- * The outputs hold a valid result afterwards.  *chosen (nullable) describes
- * the chosen plan, *best_ms (nullable) its time per call.  Not during
- * stream capture. */
+ * below on the caller's data with each candidate configuration -- of the
+ * fused path (kernel form, block and ring shape, sample size, segment size),
+ * or with RADIK_PLAIN of the multi-pass path (digit width and pass count of
+ * its candidate passes) -- `reps` timed calls each, and keeps the fastest for
+ * this batch shape (task_lens, k, flags, index width) in ws and in the
+ * process-wide tuning table below; later calls with that shape, in any
+ * workspace, use it.  The outputs hold a valid result afterwards.  *chosen
+ * (nullable) describes the chosen plan, *best_ms (nullable) its time per
+ * call.  Not during stream capture. */
 int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_bytes, const float* d_val_in,
                       const void* d_idx_in, const int64_t* h_task_lens, int64_t num_tasks, int64_t k,
                       uint32_t flags, void* stream, int reps, radik_plan_info* chosen, double* best_ms);
+
+/* Tuning table (engine-specific, no reference counterpart).  The autotuner's
+ * choice for a batch shape (task lengths, k, flags, index width) is kept for
+ * every workspace of the process: a workspace that meets a tuned shape uses
+ * it without timing again.  radik_tune_save writes the table to a text file,
+ * radik_tune_load merges one in (*entries, nullable: lines read),
+ * radik_tune_clear empties it.  With RADIK_TUNE_FILE set, that file is loaded
+ * at first use and rewritten after each autotuning.  No device work. */
+int radik_tune_save(const char* path);
+int radik_tune_load(const char* path, int64_t* entries);
+int radik_tune_clear(void);
 
 /* topk_radix_select!(val_out, idx_out, ws, val_in, idx_in, task_lens, k,
  *                    Val(LARGEST), Val(ASCEND), Val(WITHSCALE), Val(WITHIDXIN),

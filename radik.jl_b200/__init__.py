@@ -29,7 +29,8 @@ from ._lib import (RADIK_ASCEND, RADIK_ASYNC, RADIK_LARGEST, RADIK_PLAIN, RADIK_
                    RADIK_WITHPACKING, RADIK_WITHSCALE, RadiKError, check, load)
 
 __all__ = ["topk", "topk_", "topk_radix_select_", "RadiKWorkspace", "RadiKError", "topk_host",
-           "count_bin_ex", "count_bin", "select_bin", "filter_", "version", "Server"]
+           "count_bin_ex", "count_bin", "select_bin", "filter_", "version", "Server",
+           "tune_save", "tune_load", "tune_clear"]
 
 
 def _torch():
@@ -39,6 +40,27 @@ def _torch():
 
 def version() -> str:
     return load().radik_version().decode()
+
+
+def tune_save(path) -> None:
+    """Write the process-wide tuning table (the autotuner's choices by batch
+    shape, from every workspace) to a text file (radik_tune_save)."""
+    check(load().radik_tune_save(str(path).encode()))
+
+
+def tune_load(path) -> int:
+    """Merge a tuning table written by tune_save; returns the entries read.
+    Workspaces then use those choices for matching batch shapes without
+    autotuning (radik_tune_load)."""
+    n = ctypes.c_int64()
+    check(load().radik_tune_load(str(path).encode(), ctypes.byref(n)))
+    return int(n.value)
+
+
+def tune_clear() -> None:
+    """Forget every remembered tuning choice of the process (workspaces keep
+    their own)."""
+    check(load().radik_tune_clear())
 
 
 def _ptr(t) -> ctypes.c_void_p | None:
@@ -167,16 +189,18 @@ class RadiKWorkspace:
 
     def autotune(self, val_out, idx_out, val_in, idx_in, task_lens, k: int, largest: bool = True,
                  ascend: bool = True, withscale: bool = False, withidxin: bool = False, *, reps: int = 5,
-                 stream=None) -> dict:
-        """Time the fused path's candidate configurations on this batch and
-        keep the fastest for its shape (radik_ws_autotune); returns the chosen
-        plan with its time per call ("ms")."""
+                 stream=None, plain: bool = False) -> dict:
+        """Time the candidate configurations on this batch -- of the fused
+        path, or with plain=True the multi-pass path's digit schedules -- and
+        keep the fastest for its shape, here and in the process-wide tuning
+        table (radik_ws_autotune); returns the chosen plan with its time per
+        call ("ms")."""
         from ._lib import PlanInfo
         lens = _lens_array(task_lens)
         _check_io(val_out, idx_out, val_in, idx_in, lens, k, withidxin)
         info = PlanInfo()
         ms = ctypes.c_double()
-        flags = _flags(largest, ascend, withscale, withidxin)
+        flags = _flags(largest, ascend, withscale, withidxin, plain=plain)
         check(load().radik_ws_autotune(self._h, _ptr(val_out), _ptr(idx_out), _idx_bytes(idx_out.dtype), _ptr(val_in),
                                        _ptr(idx_in) if withidxin else None, lens.ctypes.data_as(ctypes.c_void_p),
                                        len(lens), int(k), flags, _stream(stream), int(reps), ctypes.byref(info),

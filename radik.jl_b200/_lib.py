@@ -33,6 +33,7 @@ EXPORTS = (
     "radik_topk_radix_select", "radik_topk", "radik_topk_host", "radik_topk_noalloc",
     "radik_count_bin_ex", "radik_count_bin", "radik_select_bin", "radik_filter",
     "radik_last_error", "radik_status_string", "radik_version", "radik_alloc_count",
+    "radik_tune_save", "radik_tune_load", "radik_tune_clear",
     "radik_server_create", "radik_server_destroy", "radik_server_submit", "radik_server_wait",
     "radik_server_get_stats", "radik_server_get_latencies", "radik_server_get_batches", "radik_server_reset_stats",
 )
@@ -106,6 +107,9 @@ def _declare(L: ctypes.CDLL) -> None:
     L.radik_server_get_batches.argtypes = [P, ctypes.POINTER(ServerBatch), I64, ctypes.POINTER(I64)]
     L.radik_server_reset_stats.argtypes = [P]
     L.radik_alloc_count.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
+    L.radik_tune_save.argtypes = [ctypes.c_char_p]
+    L.radik_tune_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(I64)]
+    L.radik_tune_clear.argtypes = []
     L.radik_last_error.restype = ctypes.c_char_p
     L.radik_status_string.restype = ctypes.c_char_p
     L.radik_status_string.argtypes = [I]

@@ -175,11 +175,33 @@ struct TuneConfig {
     int seg_div = 3;        // work items per resident block when splitting tasks
     int defer = -1;         // deferred finish of single-segment tasks: -1 automatic, 0 no, 1 yes
     int seg_min_tiles = 0;  // shortest segment of a split task in 2048-element tiles; 0 automatic
+    int plain_sched = 0;    // multi-pass path: digit schedule of the candidate passes (kPlainSchedules)
     bool operator==(const TuneConfig& o) const {
         return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
-               sample_max == o.sample_max && seg_div == o.seg_div &&
-               defer == o.defer && seg_min_tiles == o.seg_min_tiles;
+               sample_max == o.sample_max && seg_div == o.seg_div && defer == o.defer &&
+               seg_min_tiles == o.seg_min_tiles && plain_sched == o.plain_sched;
     }
+};
+
+// Digit schedules of the multi-pass path after its fixed 12-bit first digit
+// (composite bits 63..52): the (shift, width) of each candidate pass over the
+// remaining 52 bits, widths <= 12 (4096-bin histograms).  More bits per pass
+// mean fewer passes (each a histogram, a bin search, a compaction and a host
+// read of the "any task active" flag); fewer bits mean smaller histograms.
+struct PlainPass {
+    int sh, w;
+};
+constexpr int kPlainSchedules = 4;
+constexpr int kPlainMaxPasses = 7;
+struct PlainSchedule {
+    int n;
+    PlainPass pass[kPlainMaxPasses];
+};
+constexpr PlainSchedule kPlainSchedule[kPlainSchedules] = {
+    {5, {{40, 12}, {32, 8}, {20, 12}, {8, 12}, {0, 8}}},                    // score 12+8, position 12+12+8
+    {5, {{40, 12}, {28, 12}, {16, 12}, {4, 12}, {0, 4}}},                   // 12-bit digits
+    {5, {{41, 11}, {30, 11}, {19, 11}, {8, 11}, {0, 8}}},                   // 11-bit digits
+    {7, {{44, 8}, {36, 8}, {28, 8}, {20, 8}, {12, 8}, {4, 8}, {0, 4}}},    // 8-bit digits
 };
 
 TuneConfig with_env(TuneConfig c) {
@@ -191,7 +213,9 @@ TuneConfig with_env(TuneConfig c) {
     c.seg_div = std::max(1, env_int("RADIK_SEG_DIV", c.seg_div));
     c.defer = env_int("RADIK_DEFER", c.defer);
     c.seg_min_tiles = std::max(0, env_int("RADIK_SEG_MIN", c.seg_min_tiles));
+    c.plain_sched = env_int("RADIK_PLAIN_SCHED", c.plain_sched);
     if (c.sample_max != 2048 && c.sample_max != 4096) c.sample_max = 2048;
+    if (c.plain_sched < 0 || c.plain_sched >= kPlainSchedules) c.plain_sched = 0;
     return c;
 }
 
@@ -635,13 +659,141 @@ bool key_matches(const PlanKey& q, const int64_t* lens, int64_t T, int64_t k, ui
            std::equal(q.lens.begin(), q.lens.end(), lens);
 }
 
+// Process-wide tuning table: the autotuner's choices for every batch shape it
+// has seen (any workspace), keyed by the shape's digest; saved to and loaded
+// from a text file (radik_tune_save / radik_tune_load, or the file named by
+// RADIK_TUNE_FILE, read at first use and rewritten after each autotuning).
+struct TuneEntry {
+    uint64_t digest = 0;  // FNV-1a of the task lengths
+    int64_t T = 0, N = 0, k = 0;
+    uint32_t flags = 0;
+    int idx_bytes = 0;
+    TuneConfig cfg;
+};
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune;
+std::once_flag g_tune_env_once;
+
+uint64_t lens_digest(const int64_t* lens, int64_t T) {
+    uint64_t h = 1469598103934665603ull;
+    for (int64_t t = 0; t < T; ++t) {
+        uint64_t v = static_cast<uint64_t>(lens[t]);
+        for (int b = 0; b < 8; ++b) {
+            h ^= (v >> (8 * b)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    }
+    return h;
+}
+
+TuneEntry tune_entry(const int64_t* lens, int64_t T, int64_t k, uint32_t mflags, int idx_bytes) {
+    TuneEntry e;
+    e.digest = lens_digest(lens, T);
+    e.T = T;
+    e.N = std::accumulate(lens, lens + T, int64_t(0));
+    e.k = k;
+    e.flags = mflags;
+    e.idx_bytes = idx_bytes;
+    return e;
+}
+
+bool same_shape(const TuneEntry& a, const TuneEntry& b) {
+    return a.digest == b.digest && a.T == b.T && a.N == b.N && a.k == b.k && a.flags == b.flags &&
+           a.idx_bytes == b.idx_bytes;
+}
+
+// One line per entry: digest T N k flags idx_bytes, then the configuration.
+int tune_write(const char* path) {
+    std::FILE* fp = std::fopen(path, "w");
+    if (!fp) return -1;
+    std::fprintf(fp, "# radik tuning table v1: digest T N k flags idx_bytes form ws_threads ws_j ws_stages "
+                     "sample_max seg_div defer seg_min_tiles plain_sched\n");
+    int n = 0;
+    for (const TuneEntry& e : g_tune) {
+        const TuneConfig& c = e.cfg;
+        std::fprintf(fp, "%llu %lld %lld %lld %u %d %d %d %d %d %d %d %d %d %d\n",
+                     static_cast<unsigned long long>(e.digest), static_cast<long long>(e.T),
+                     static_cast<long long>(e.N), static_cast<long long>(e.k), e.flags, e.idx_bytes, c.form,
+                     c.ws_threads, c.ws_j, c.ws_stages, c.sample_max, c.seg_div, c.defer, c.seg_min_tiles,
+                     c.plain_sched);
+        ++n;
+    }
+    return std::fclose(fp) == 0 ? n : -1;
+}
+
+void tune_put(const TuneEntry& e) {
+    for (TuneEntry& x : g_tune)
+        if (same_shape(x, e)) {
+            x.cfg = e.cfg;
+            return;
+        }
+    g_tune.push_back(e);
+}
+
+// Reads a table written by tune_write; malformed lines are skipped.  Returns
+// the entries read, -1 when the file cannot be opened.
+int tune_read(const char* path) {
+    std::FILE* fp = std::fopen(path, "r");
+    if (!fp) return -1;
+    char line[512];
+    int n = 0;
+    while (std::fgets(line, sizeof(line), fp)) {
+        if (line[0] == '#') continue;
+        unsigned long long dg = 0;
+        long long T = 0, N = 0, k = 0;
+        unsigned flags = 0;
+        TuneEntry e;
+        TuneConfig& c = e.cfg;
+        if (std::sscanf(line, "%llu %lld %lld %lld %u %d %d %d %d %d %d %d %d %d %d", &dg, &T, &N, &k, &flags,
+                        &e.idx_bytes, &c.form, &c.ws_threads, &c.ws_j, &c.ws_stages, &c.sample_max, &c.seg_div,
+                        &c.defer, &c.seg_min_tiles, &c.plain_sched) != 15)
+            continue;
+        if (c.plain_sched < 0 || c.plain_sched >= kPlainSchedules) continue;
+        e.digest = dg;
+        e.T = T;
+        e.N = N;
+        e.k = k;
+        e.flags = flags;
+        tune_put(e);
+        ++n;
+    }
+    std::fclose(fp);
+    return n;
+}
+
+void tune_env_load() {
+    std::call_once(g_tune_env_once, [] {
+        const char* path = std::getenv("RADIK_TUNE_FILE");
+        if (path && *path) {
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            tune_read(path);
+        }
+    });
+}
+
 // The configuration for a batch shape: the one radik_ws_autotune chose for
-// it, else the defaults; environment overrides on top.
+// it in this workspace, else in any workspace of the process (or a loaded
+// table), else the defaults; environment overrides on top.
 TuneConfig shape_config(const radik_ws* ws, const int64_t* lens, int64_t T, int64_t k, uint32_t mflags,
                         int idx_bytes) {
     TuneConfig tc;
+    bool found = false;
     for (const auto& e : ws->tuned)
-        if (key_matches(e.first, lens, T, k, mflags, idx_bytes)) { tc = e.second; break; }
+        if (key_matches(e.first, lens, T, k, mflags, idx_bytes)) {
+            tc = e.second;
+            found = true;
+            break;
+        }
+    if (!found) {
+        tune_env_load();
+        const TuneEntry q = tune_entry(lens, T, k, mflags, idx_bytes);
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (const TuneEntry& e : g_tune)
+            if (same_shape(e, q)) {
+                tc = e.cfg;
+                break;
+            }
+    }
     return with_env(tc);
 }
 
@@ -928,10 +1080,10 @@ int run_plain(radik_ws* ws, const FusedParams& fp, uint32_t flags, cudaStream_t 
     // Candidate passes over the remaining composite bits; the host reads the
     // "any task active" flag after each pass (src/algorithm.jl:242-244,
     // :275-277 read back candidate counts the same way).
-    static const int kSh[5] = {40, 32, 20, 8, 0};
-    static const int kW[5] = {12, 8, 12, 12, 8};
+    const PlainSchedule& sched = kPlainSchedule[pl.key.tune.plain_sched];
     int src = 0;
-    for (int ps = 0; ps < 5; ++ps) {
+    for (int ps = 0; ps < sched.n; ++ps) {
+        const int sh = sched.pass[ps].sh, wd = sched.pass[ps].w;
         uint32_t h_any = 0;
         RADIK_CUDA(cudaMemcpyAsync(&h_any, any, 4, cudaMemcpyDeviceToHost, s));
         RADIK_CUDA(cudaStreamSynchronize(s));
@@ -942,12 +1094,12 @@ int run_plain(radik_ws* ws, const FusedParams& fp, uint32_t flags, cudaStream_t 
             1, std::min<int64_t>((maxlen + 255) / 256, std::max<int64_t>(1, 4LL * di.sms / std::max<int64_t>(T, 1)))));
         for (int64_t t0 = 0; t0 < T; t0 += 65535) {
             unsigned gy = static_cast<unsigned>(std::min<int64_t>(65535, T - t0));
-            plain_hist_cand<256><<<dim3(gx, gy), 256, 0, s>>>(p, static_cast<int>(t0), src, kSh[ps], kW[ps]);
+            plain_hist_cand<256><<<dim3(gx, gy), 256, 0, s>>>(p, static_cast<int>(t0), src, sh, wd);
         }
-        plain_select<256><<<static_cast<unsigned>(T), 256, 0, s>>>(p, ps + 1, kW[ps]);
+        plain_select<256><<<static_cast<unsigned>(T), 256, 0, s>>>(p, ps + 1, wd);
         for (int64_t t0 = 0; t0 < T; t0 += 65535) {
             unsigned gy = static_cast<unsigned>(std::min<int64_t>(65535, T - t0));
-            plain_compact_cand<256><<<dim3(gx, gy), 256, 0, s>>>(p, static_cast<int>(t0), src, kSh[ps], kW[ps]);
+            plain_compact_cand<256><<<dim3(gx, gy), 256, 0, s>>>(p, static_cast<int>(t0), src, sh, wd);
         }
         RADIK_CUDA(cudaMemsetAsync(any, 0, 4, s));
         plain_advance<<<static_cast<unsigned>((T + 255) / 256), 256, 0, s>>>(p, any);
@@ -1093,6 +1245,30 @@ int radik_ws_error(radik_ws* ws, uint32_t* bits) {
     return RADIK_OK;
 }
 
+int radik_tune_save(const char* path) {
+    if (!path) return fail(RADIK_ERR_INVALID, "NULL path");
+    tune_env_load();
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    if (tune_write(path) < 0) return fail(RADIK_ERR_INVALID, "cannot write the tuning file");
+    return RADIK_OK;
+}
+
+int radik_tune_load(const char* path, int64_t* entries) {
+    if (!path) return fail(RADIK_ERR_INVALID, "NULL path");
+    tune_env_load();
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    const int n = tune_read(path);
+    if (n < 0) return fail(RADIK_ERR_INVALID, "cannot read the tuning file");
+    if (entries) *entries = n;
+    return RADIK_OK;
+}
+
+int radik_tune_clear(void) {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune.clear();
+    return RADIK_OK;
+}
+
 int radik_ws_plan_info(const radik_ws* ws, radik_plan_info* info) {
     if (!ws || !info) return fail(RADIK_ERR_INVALID, "NULL argument");
     const Plan& pl = ws->plan;
@@ -1185,7 +1361,6 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
                       void* stream, int reps, radik_plan_info* chosen, double* best_ms) {
     if (!ws || !h_task_lens) return fail(RADIK_ERR_INVALID, "NULL argument");
     if (num_tasks <= 0 || k <= 0) return fail(RADIK_ERR_INVALID, "num_tasks and k must be positive");
-    if (flags & RADIK_PLAIN) return fail(RADIK_ERR_INVALID, "the multi-pass path has nothing to tune");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaStreamCaptureStatus capst = cudaStreamCaptureStatusNone;
     RADIK_CUDA(cudaStreamIsCapturing(s, &capst));
@@ -1199,6 +1374,14 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     std::vector<TuneConfig> cands;
     TuneConfig d;
     cands.push_back(d);
+    if (flags & RADIK_PLAIN) {
+        // The multi-pass path: its digit schedules.
+        for (int i = 1; i < kPlainSchedules; ++i) {
+            TuneConfig c = d;
+            c.plain_sched = i;
+            cands.push_back(c);
+        }
+    } else {
     { TuneConfig c = d; c.form = 1; c.ws_stages = 12; cands.push_back(c); }
     { TuneConfig c = d; c.form = 1; c.ws_threads = 256; c.ws_stages = 16; cands.push_back(c); }
     { TuneConfig c = d; c.form = 1; c.sample_max = 4096; cands.push_back(c); }
@@ -1212,6 +1395,7 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     { TuneConfig c = d; c.defer = 1; cands.push_back(c); }
     { TuneConfig c = d; c.seg_min_tiles = 4; cands.push_back(c); }
     { TuneConfig c = d; c.seg_min_tiles = 64; cands.push_back(c); }
+    }
     PlanKey base = plan_key(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
     auto set_choice = [&](const TuneConfig& c) {
         for (auto& e : ws->tuned) {
@@ -1252,6 +1436,17 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     cudaEventDestroy(e1);
     if (best >= 1e30) return rc != RADIK_OK ? rc : fail(RADIK_ERR_INVALID, "no configuration ran");
     set_choice(best_c);
+    {
+        // Remember the choice for every workspace of the process (and the
+        // tuning file, when one is named).
+        tune_env_load();
+        TuneEntry e = tune_entry(h_task_lens, num_tasks, k, base.flags, idx_bytes);
+        e.cfg = best_c;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        tune_put(e);
+        const char* path = std::getenv("RADIK_TUNE_FILE");
+        if (path && *path) tune_write(path);
+    }
     rc = build_plan(ws, h_task_lens, num_tasks, k, flags, idx_bytes);
     if (rc) return rc;
     if (chosen) radik_ws_plan_info(ws, chosen);

@@ -173,3 +173,90 @@ def test_autotune_keeps_results_exact(oracle, radik, torch_cuda):
         assert np.array_equal(io.cpu().numpy().astype(np.int64), oi.astype(np.int64))
         assert ws.plan_info()["path"] == info["path"]
     ws.close()
+
+
+def _tuned_lines(path):
+    return [l.split() for l in path.read_text().splitlines() if l and not l.startswith("#")]
+
+
+def test_tuning_table_shared_across_workspaces(oracle, radik, torch_cuda, tmp_path):
+    """The autotuner's choice for a batch shape is kept process-wide: a new
+    workspace meeting that shape uses it without timing; a saved and edited
+    table, loaded back, decides the plan of the next workspace."""
+    torch = torch_cuda
+    radik.tune_clear()
+    rng = np.random.default_rng(123)
+    lens = [40_000] * 24 + [300_000, 7]
+    k = 128
+    h = rng.standard_normal(sum(lens)).astype(np.float32)
+    x = torch.from_numpy(h).cuda()
+    vo = torch.empty((len(lens), k), device="cuda")
+    io = torch.empty((len(lens), k), dtype=torch.int32, device="cuda")
+    ov, oi = oracle.topk(h, lens, k)
+    ws = radik.RadiKWorkspace("cuda", max(lens), len(lens))
+    info = ws.autotune(vo, io, x, None, lens, k, True, True, reps=2)
+    ws.close()
+    p = tmp_path / "tune.txt"
+    radik.tune_save(p)
+    rows = _tuned_lines(p)
+    assert len(rows) == 1 and int(rows[0][1]) == len(lens) and int(rows[0][2]) == sum(lens) and int(rows[0][3]) == k
+
+    def run_new():
+        w = radik.RadiKWorkspace("cuda", max(lens), len(lens))
+        vo.fill_(7.0)
+        radik.topk_radix_select_(vo, io, w, x, None, lens, k, True, True)
+        assert np.array_equal(vo.cpu().numpy().view(np.uint32), ov.view(np.uint32))
+        assert np.array_equal(io.cpu().numpy().astype(np.int64), oi.astype(np.int64))
+        plan = w.plan_info()
+        w.close()
+        return plan
+
+    assert run_new()["path"] == info["path"]
+    for form, path in ((0, 0), (1, 1)):
+        rows[0][6] = str(form)  # the kernel form field
+        p2 = tmp_path / f"tune_{form}.txt"
+        p2.write_text(" ".join(rows[0]) + "\n")
+        radik.tune_clear()
+        assert radik.tune_load(p2) == 1
+        assert run_new()["path"] == path
+    radik.tune_clear()
+
+
+def test_plain_path_digit_schedules(oracle, radik, torch_cuda, tmp_path):
+    """The multi-pass path tunes its digit schedule (pass widths and count);
+    every schedule gives the oracle's rows, ties and NaNs included."""
+    torch = torch_cuda
+    radik.tune_clear()
+    rng = np.random.default_rng(321)
+    lens = [100_000, 3, 0, 65_536, 250_000]
+    k = 300
+    h = rng.integers(-50, 50, sum(lens)).astype(np.float32)  # many ties
+    h[::101] = np.nan
+    x = torch.from_numpy(h).cuda()
+    vo = torch.empty((len(lens), k), device="cuda")
+    io = torch.empty((len(lens), k), dtype=torch.int64, device="cuda")
+    for largest, ascend in ((True, False), (False, True)):
+        ov, oi = oracle.topk(h, lens, k, largest=largest, rev=not ascend)
+        ws = radik.RadiKWorkspace("cuda", max(lens), len(lens))
+        info = ws.autotune(vo, io, x, None, lens, k, largest, ascend, reps=1, plain=True)
+        assert info["path"] == 2
+        ws.close()
+        p = tmp_path / "plain.txt"
+        radik.tune_save(p)
+        rows = [r for r in _tuned_lines(p) if int(r[1]) == len(lens)]
+        assert len(rows) == 1
+        for sched in range(4):
+            rows[0][14] = str(sched)
+            p2 = tmp_path / f"plain_{sched}.txt"
+            p2.write_text(" ".join(rows[0]) + "\n")
+            radik.tune_clear()
+            assert radik.tune_load(p2) == 1
+            w = radik.RadiKWorkspace("cuda", max(lens), len(lens))
+            vo.fill_(7.0)
+            radik.topk_radix_select_(vo, io, w, x, None, lens, k, largest, ascend, plain=True)
+            got_v = vo.cpu().numpy()
+            assert np.array_equal(got_v.view(np.uint32), ov.view(np.uint32)), sched
+            assert np.array_equal(io.cpu().numpy(), oi.astype(np.int64)), sched
+            assert w.plan_info()["path"] == 2
+            w.close()
+        radik.tune_clear()
