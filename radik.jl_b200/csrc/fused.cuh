@@ -257,8 +257,8 @@ __device__ void finish_task(const FusedParams& p, const TaskView& tv, uint64_t* 
         regs_sort_u64<THREADS, 2>(buf, m, buf + 2 * THREADS);
     } else if (m <= 4u * THREADS && p.cap >= 12u * THREADS) {
         regs_sort_u64<THREADS, 4>(buf, m, buf + 4 * THREADS);
-    } else if (THREADS <= 256 && m <= 8u * THREADS && p.cap >= 24u * THREADS) {
-        regs_sort_u64<THREADS, (THREADS <= 256 ? 8 : 1)>(buf, m, buf + 8 * THREADS);
+    } else if (m <= 8u * THREADS && p.cap >= 24u * THREADS) {
+        regs_sort_u64<THREADS, 8>(buf, m, buf + 8 * THREADS);
     } else if (m <= kBitonicMax) {
         uint32_t P = 1;
         while (P < m) P <<= 1;

@@ -117,6 +117,42 @@ __global__ void __launch_bounds__(THREADS) merge_topk_kernel(FusedParams p, cons
         }
         return;
     }
+    if (n >= k && spill_off + kWarpBisect <= cap && hist_off + k <= cap) {
+        // The region fits beside the select's scratch: load it at once, find
+        // the k-th largest composite (block_topk_bound), gather the k entries
+        // at or above it in the staging area behind the histograms, move them
+        // to the front and sort and write them (finish_task).
+        uint64_t vor = 0, vand = ~0ull;
+#pragma unroll 8
+        for (uint32_t i = tid; i < n; i += THREADS) {
+            const uint64_t c = __ldcg(src + i);
+            s_buf[i] = c;
+            vor |= c;
+            vand &= c;
+        }
+        block_or_and<THREADS>(vor, vand, sh.bs);  // barriers: the region is in s_buf
+        const uint64_t tau = block_topk_bound<THREADS>(s_buf, n, k, vor, vand, sh.bs,
+                                                       reinterpret_cast<uint32_t*>(s_buf + hist_off),
+                                                       s_buf + spill_off, &s_spill_n, &s_tau, p.err);
+        uint64_t* stage = s_buf + hist_off;  // [hist_off, hist_off + k) does not meet [0, k): k <= n < hist_off
+        uint32_t nsel = 0;
+        for (uint32_t i = tid; i < n; i += THREADS) nsel += (s_buf[i] >= tau) ? 1u : 0u;
+        uint32_t total = 0;
+        uint32_t slot = block_exclusive_scan<THREADS>(nsel, &total, sh.bs);  // barriers: histograms no longer read
+        for (uint32_t i = tid; i < n; i += THREADS) {
+            const uint64_t c = s_buf[i];
+            if (c < tau) continue;
+            if (slot < k) stage[slot] = c;
+            else record_error(p.err, kErrInternal);
+            ++slot;
+        }
+        block_sync<THREADS>();
+        for (uint32_t i = tid; i < k; i += THREADS) s_buf[i] = stage[i];
+        if (tid == 0 && total != k) record_error(p.err, kErrInternal);
+        block_sync<THREADS>();
+        finish_task<THREADS, !kScale>(p, tv, s_buf, k, sh);
+        return;
+    }
     for (uint32_t b0 = 0; b0 < n;) {
         const uint32_t cnt = sh.cnt;
         const uint32_t take = min(n - b0, cap - cnt);  // > 0: cnt <= mid_keep < cap
