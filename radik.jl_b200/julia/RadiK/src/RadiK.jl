@@ -210,6 +210,21 @@ function alloc_count()
     return n[]
 end
 
+# Tuning table: the autotuner's choices by batch shape, shared by every
+# workspace of the process, kept in a text file between processes.
+"""Write the process-wide tuning table to `path`."""
+tune_save(path::AbstractString) = (check(ccall((:radik_tune_save, LIB), Cint, (Cstring,), path)); nothing)
+
+"""Merge a tuning table written by `tune_save`; returns the entries read."""
+function tune_load(path::AbstractString)
+    n = Ref{Int64}(0)
+    check(ccall((:radik_tune_load, LIB), Cint, (Cstring, Ptr{Int64}), path, n))
+    return n[]
+end
+
+"""Forget every remembered tuning choice of the process."""
+tune_clear() = (check(ccall((:radik_tune_clear, LIB), Cint, ())); nothing)
+
 # Request server: continuous batching of independent top-k requests.
 struct ServerConfig
     slots::Cint
