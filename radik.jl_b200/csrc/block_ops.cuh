@@ -631,6 +631,8 @@ __device__ __forceinline__ void bitonic_sort_u64(uint64_t* a, uint32_t n, bool d
 // and a scatter in which every warp walks its chunk in order, 32 keys at a
 // time, ranking lanes of equal digits with one match: no block barrier
 // inside the scatter, five per pass.
+constexpr int kSortGroups = 4;  // radix_sort_u64: groups of 32 keys a warp handles at once
+
 template <int THREADS>
 __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, uint32_t n, BlockScratch<THREADS>& s,
                                     uint32_t* warp_digit /* [THREADS/32][256] shared */,
@@ -648,12 +650,22 @@ __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, ui
     uint32_t* mine = warp_digit + w * 256;
     for (int sh = 0; sh < 64; sh += 8) {
         if (((diff >> sh) & 0xffull) == 0) continue;
-        // 1. histogram of this warp's chunk
+        // 1. histogram of this warp's chunk, four groups of 32 keys at a time
+        //    (their loads and matches in flight together)
         for (uint32_t j = lane; j < 256; j += 32) mine[j] = 0;
         __syncwarp();
-        for (uint32_t base = lo; base < hi; base += 32) {
-            const uint32_t i = base + lane;
-            warp_hist_add(mine, i < hi ? static_cast<uint32_t>((a[i] >> sh) & 0xff) : 0u, i < hi);
+        for (uint32_t base = lo; base < hi; base += 32u * kSortGroups) {
+            uint32_t d[kSortGroups];
+#pragma unroll
+            for (int u = 0; u < kSortGroups; ++u) {
+                const uint32_t i = base + static_cast<uint32_t>(u) * 32u + lane;
+                d[u] = i < hi ? static_cast<uint32_t>((a[i] >> sh) & 0xff) : 256u + lane;
+            }
+#pragma unroll
+            for (int u = 0; u < kSortGroups; ++u) {
+                const uint32_t peers = __match_any_sync(kFullMask, d[u]);
+                if (d[u] < 256u && (lanemask_lt() & peers) == 0u) atomicAdd(mine + d[u], static_cast<uint32_t>(__popc(peers)));
+            }
         }
         block_sync<THREADS>();
         // 2. digit totals, their exclusive scan, then each warp's first slot
@@ -681,19 +693,31 @@ __device__ __forceinline__ uint64_t* radix_sort_u64(uint64_t* a, uint64_t* b, ui
             }
         }
         block_sync<THREADS>();
-        // 3. stable scatter: chunks in warp order, keys in order inside a chunk
-        for (uint32_t base = lo; base < hi; base += 32) {
-            const uint32_t i = base + lane;
-            const bool valid = i < hi;
-            const uint64_t v = valid ? a[i] : 0ull;
-            const uint32_t d = valid ? static_cast<uint32_t>((v >> sh) & 0xff) : 256u + lane;
-            const uint32_t peers = __match_any_sync(kFullMask, d);
-            const uint32_t below = peers & lanemask_lt();
-            const uint32_t off = valid ? mine[d] : 0u;
-            if (valid) b[off + __popc(below)] = v;
-            __syncwarp();
-            if (valid && below == 0u) mine[d] = off + __popc(peers);  // the first lane of each digit advances it
-            __syncwarp();
+        // 3. stable scatter: chunks in warp order, keys in order inside a
+        //    chunk.  Per group of 32 keys the first lane of each digit takes
+        //    the group's slots with one shared atomic on the warp's cursor and
+        //    hands the base to its peers; a warp barrier after each group's
+        //    atomics orders them before the next group's, so keys keep their
+        //    order.  The groups' loads and matches are in flight together.
+        for (uint32_t base = lo; base < hi; base += 32u * kSortGroups) {
+            uint64_t v[kSortGroups];
+            uint32_t d[kSortGroups];
+#pragma unroll
+            for (int u = 0; u < kSortGroups; ++u) {
+                const uint32_t i = base + static_cast<uint32_t>(u) * 32u + lane;
+                v[u] = i < hi ? a[i] : 0ull;
+                d[u] = i < hi ? static_cast<uint32_t>((v[u] >> sh) & 0xff) : 256u + lane;
+            }
+#pragma unroll
+            for (int u = 0; u < kSortGroups; ++u) {
+                const uint32_t peers = __match_any_sync(kFullMask, d[u]);
+                const uint32_t leader = static_cast<uint32_t>(__ffs(peers)) - 1u;
+                uint32_t off = 0;
+                if (d[u] < 256u && lane == leader) off = atomicAdd(mine + d[u], static_cast<uint32_t>(__popc(peers)));
+                __syncwarp();
+                off = __shfl_sync(kFullMask, off, static_cast<int>(leader));
+                if (d[u] < 256u) b[off + __popc(peers & lanemask_lt())] = v[u];
+            }
         }
         block_sync<THREADS>();
         uint64_t* t = a; a = b; b = t;
