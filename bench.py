@@ -2,7 +2,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--config uniform_batch|adversarial_single|uneven_batch|single_1m|
-                              rows64_k8192|serving] [--tune-file PATH]
+                              rows64_k8192|rows256_k8192|serving] [--tune-file PATH]
 
 A step is one batched top-k over the configuration's synthetic input (seeded,
 shapes and distributions of the workload; no dataset exists):
@@ -17,6 +17,8 @@ shapes and distributions of the workload; no dataset exists):
   single_1m           one task of 2^20 N(0,1) (seed 0), k=100, largest
   rows64_k8192        64 tasks x 2^20 N(0,1), k=8192, largest (the serving
                       stream's heaviest request shape)
+  rows256_k8192       256 tasks x 32,768 N(0,1), k=8192, largest (its
+                      costliest shape per element)
   serving             the request server on a Poisson stream of top-k requests
                       (see run_serving)
 `value` is elements/s with the inputs already in HBM (timed with CUDA events
@@ -81,6 +83,9 @@ CONFIGS = {
     # The serving stream's heaviest request shape: 64 rows of 2^20 N(0,1),
     # k = 8192 (sampled thresholds, the merge and rank kernels, radix sorts).
     "rows64_k8192": dict(k=8192, largest=True, rev=False, custom_idx=False),
+    # The serving stream's costliest shape per element: 256 rows of 32,768
+    # N(0,1), k = 8192 (a quarter of each row; the barrier form and its sort).
+    "rows256_k8192": dict(k=8192, largest=True, rev=False, custom_idx=False),
 }
 
 
@@ -93,6 +98,8 @@ def task_lens_of(name: str) -> list[int]:
         return [1 << 20]
     if name == "rows64_k8192":
         return [1 << 20] * 64
+    if name == "rows256_k8192":
+        return [1 << 15] * 256
     rng = np.random.default_rng(3)
     v = np.clip(np.round(rng.lognormal(np.log(20000), 1.5, size=4096)), 1, 4_194_304)
     return [int(x) for x in v]
@@ -233,6 +240,9 @@ def run_reference(args, rank: int, world: int):
     elif args.config == "rows64_k8192":
         sample_lens = lens[:4]
         sample = "4 of the 64 rows per step"
+    elif args.config == "rows256_k8192":
+        sample_lens = lens[:32]
+        sample = "32 of the 256 rows per step"
     else:
         sample_lens = lens[:256]
         sample = "the first 256 of the 4096 tasks per step"
@@ -304,6 +314,8 @@ def cpu_baseline_quick(args, config: str) -> dict:
         sl, sample = lens, "the whole 2^20-element task, 3 repetitions"
     elif config == "rows64_k8192":
         sl, sample = lens[:4], "4 of the 64 rows, 3 repetitions"
+    elif config == "rows256_k8192":
+        sl, sample = lens[:32], "32 of the 256 rows, 3 repetitions"
     else:
         sl, sample = lens[:256], "first 256 of the 4096 tasks, 3 repetitions"
     N = int(sum(sl))
