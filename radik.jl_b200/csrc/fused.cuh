@@ -561,8 +561,13 @@ __device__ void finish_candidates(const FusedParams& p, const TaskView& tv, uint
 
 // Starting threshold of a single-segment task from a sample of `S` of its
 // elements (16 chunks of S/16 consecutive elements): one below the composite
-// of sample rank r, where r is chosen so that about 2k elements of the task
-// are expected above it.  0 (no pruning) when the sample is too small.
+// of sample rank r.  With lam = k S / len sampled elements expected among the
+// task's k best, r = lam + 5 sqrt(lam) + 12 puts the threshold five standard
+// deviations of that count below the k-th (too high only with probability
+// ~1e-7; the task is then redone without it).  Up to r = S / 2, so a k that
+// is a quarter of the row (lam = S / 4) still gets a threshold near the
+// sample's 66th percentile instead of none.  0 (no pruning) when the sample
+// is too small.
 template <int THREADS, bool kScale>
 __device__ uint64_t sampled_threshold(const TaskView& tv, float scaler, uint32_t k, uint64_t* buf,
                                       FusedShared<THREADS>& sh, uint32_t* err) {
@@ -570,8 +575,8 @@ __device__ uint64_t sampled_threshold(const TaskView& tv, float scaler, uint32_t
     const int64_t len = tv.len;
     if (len < 8 * static_cast<int64_t>(S)) return 0ull;
     const float lam = static_cast<float>(k) * S / static_cast<float>(len);
-    const uint32_t r = static_cast<uint32_t>(ceilf(2.0f * lam + 4.0f * sqrtf(lam) + 12.0f));
-    if (r > S / 4) return 0ull;
+    const uint32_t r = static_cast<uint32_t>(ceilf(lam + 5.0f * sqrtf(lam) + 12.0f));
+    if (r > S / 2) return 0ull;
     const int64_t cstride = len / 16;
     uint64_t vor = 0, vand = ~0ull;
     for (uint32_t i = threadIdx.x; i < S; i += THREADS) {
