@@ -176,10 +176,11 @@ struct TuneConfig {
     int defer = -1;         // deferred finish of single-segment tasks: -1 automatic, 0 no, 1 yes
     int seg_min_tiles = 0;  // shortest segment of a split task in 2048-element tiles; 0 automatic
     int plain_sched = 0;    // multi-pass path: digit schedule of the candidate passes (kPlainSchedules)
+    int bar_threads = 0;    // barrier form's block: 256 or 512 threads; 0 automatic (512 for 4096 < k <= 8192)
     bool operator==(const TuneConfig& o) const {
         return form == o.form && ws_threads == o.ws_threads && ws_j == o.ws_j && ws_stages == o.ws_stages &&
                sample_max == o.sample_max && seg_div == o.seg_div && defer == o.defer &&
-               seg_min_tiles == o.seg_min_tiles && plain_sched == o.plain_sched;
+               seg_min_tiles == o.seg_min_tiles && plain_sched == o.plain_sched && bar_threads == o.bar_threads;
     }
 };
 
@@ -214,6 +215,8 @@ TuneConfig with_env(TuneConfig c) {
     c.defer = env_int("RADIK_DEFER", c.defer);
     c.seg_min_tiles = std::max(0, env_int("RADIK_SEG_MIN", c.seg_min_tiles));
     c.plain_sched = env_int("RADIK_PLAIN_SCHED", c.plain_sched);
+    c.bar_threads = env_int("RADIK_THREADS", c.bar_threads);
+    if (c.bar_threads != 256 && c.bar_threads != 512) c.bar_threads = 0;
     if (c.sample_max != 2048 && c.sample_max != 4096) c.sample_max = 2048;
     if (c.plain_sched < 0 || c.plain_sched >= kPlainSchedules) c.plain_sched = 0;
     return c;
@@ -494,10 +497,15 @@ int plan_shape(const int64_t* lens, int64_t T, int64_t k, uint32_t flags, Plan& 
     const size_t kk = static_cast<size_t>(k);
     const size_t smem_max = static_cast<size_t>(di.max_smem_optin) - 4096;
 
-    // Shapes.  Barrier form (fused.cuh): RADIK_THREADS x RADIK_VEC tiles.
-    // Warp-specialised form (fused_ws.cuh): RADIK_WST consumer threads,
-    // warp tiles of 128 * RADIK_WSJ elements, RADIK_WSS ring stages.
-    const int bar_threads = env_int("RADIK_THREADS", 256);
+    // Shapes.  Barrier form (fused.cuh): bar_threads x RADIK_VEC tiles, 512
+    // threads for 4096 < k <= 8192 (their final selection and sort of up to
+    // 16 keys per thread: 256 x 32,768 at k = 8192 0.427 -> 0.390 ms,
+    // 256 x 131,072 0.782 -> 0.682 ms, the served stream +18 %; at k = 4096
+    // 256 threads stay faster, 0.160 against 0.200 ms; beyond 8192 the
+    // 256-thread plan's choice of the multi-pass path is kept).
+    // Warp-specialised form (fused_ws.cuh): RADIK_WST consumer threads, warp
+    // tiles of 128 * RADIK_WSJ elements, RADIK_WSS ring stages.
+    const int bar_threads = tc.bar_threads != 0 ? tc.bar_threads : ((kk > 4096 && kk <= 8192) ? 512 : 256);
     const int bar_vec = env_int("RADIK_VEC", 8);
     const int ws_env = tc.form;
     const int ws_j = tc.ws_j;
@@ -707,15 +715,22 @@ int tune_write(const char* path) {
     std::FILE* fp = std::fopen(path, "w");
     if (!fp) return -1;
     std::fprintf(fp, "# radik tuning table v1: digest T N k flags idx_bytes form ws_threads ws_j ws_stages "
-                     "sample_max seg_div defer seg_min_tiles plain_sched\n");
+                     "sample_max seg_div defer seg_min_tiles plain_sched [bar_threads]\n");
     int n = 0;
     for (const TuneEntry& e : g_tune) {
         const TuneConfig& c = e.cfg;
-        std::fprintf(fp, "%llu %lld %lld %lld %u %d %d %d %d %d %d %d %d %d %d\n",
-                     static_cast<unsigned long long>(e.digest), static_cast<long long>(e.T),
-                     static_cast<long long>(e.N), static_cast<long long>(e.k), e.flags, e.idx_bytes, c.form,
-                     c.ws_threads, c.ws_j, c.ws_stages, c.sample_max, c.seg_div, c.defer, c.seg_min_tiles,
-                     c.plain_sched);
+        if (c.bar_threads != 0)
+            std::fprintf(fp, "%llu %lld %lld %lld %u %d %d %d %d %d %d %d %d %d %d %d\n",
+                         static_cast<unsigned long long>(e.digest), static_cast<long long>(e.T),
+                         static_cast<long long>(e.N), static_cast<long long>(e.k), e.flags, e.idx_bytes, c.form,
+                         c.ws_threads, c.ws_j, c.ws_stages, c.sample_max, c.seg_div, c.defer, c.seg_min_tiles,
+                         c.plain_sched, c.bar_threads);
+        else
+            std::fprintf(fp, "%llu %lld %lld %lld %u %d %d %d %d %d %d %d %d %d %d\n",
+                         static_cast<unsigned long long>(e.digest), static_cast<long long>(e.T),
+                         static_cast<long long>(e.N), static_cast<long long>(e.k), e.flags, e.idx_bytes, c.form,
+                         c.ws_threads, c.ws_j, c.ws_stages, c.sample_max, c.seg_div, c.defer, c.seg_min_tiles,
+                         c.plain_sched);
         ++n;
     }
     return std::fclose(fp) == 0 ? n : -1;
@@ -744,11 +759,14 @@ int tune_read(const char* path) {
         unsigned flags = 0;
         TuneEntry e;
         TuneConfig& c = e.cfg;
-        if (std::sscanf(line, "%llu %lld %lld %lld %u %d %d %d %d %d %d %d %d %d %d", &dg, &T, &N, &k, &flags,
-                        &e.idx_bytes, &c.form, &c.ws_threads, &c.ws_j, &c.ws_stages, &c.sample_max, &c.seg_div,
-                        &c.defer, &c.seg_min_tiles, &c.plain_sched) != 15)
-            continue;
+        const int got = std::sscanf(line, "%llu %lld %lld %lld %u %d %d %d %d %d %d %d %d %d %d %d", &dg, &T, &N, &k,
+                                    &flags, &e.idx_bytes, &c.form, &c.ws_threads, &c.ws_j, &c.ws_stages,
+                                    &c.sample_max, &c.seg_div, &c.defer, &c.seg_min_tiles, &c.plain_sched,
+                                    &c.bar_threads);
+        if (got != 15 && got != 16) continue;
+        if (got == 15) c.bar_threads = 0;
         if (c.plain_sched < 0 || c.plain_sched >= kPlainSchedules) continue;
+        if (c.bar_threads != 0 && c.bar_threads != 256 && c.bar_threads != 512) continue;
         e.digest = dg;
         e.T = T;
         e.N = N;
@@ -1389,6 +1407,7 @@ int radik_ws_autotune(radik_ws* ws, float* d_val_out, void* d_idx_out, int idx_b
     // batch of up to 7 tasks per SM.
     { TuneConfig c = d; c.form = 1; c.ws_threads = 64; c.ws_stages = 4; cands.push_back(c); }
     { TuneConfig c = d; c.form = 0; cands.push_back(c); }
+    { TuneConfig c = d; c.form = 0; c.bar_threads = (k > 4096 && k <= 8192) ? 256 : 512; cands.push_back(c); }
     { TuneConfig c = d; c.seg_div = 2; cands.push_back(c); }
     { TuneConfig c = d; c.seg_div = 6; cands.push_back(c); }
     { TuneConfig c = d; c.defer = 0; cands.push_back(c); }
